@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 em2d time step.
+
+Workload: the uniform warm plasma -- 2048x2048 cells, dx = dy = 0.1,
+dt = 0.07, periodic, 16x16 tiles, one electron species with 8x8 particles
+per cell (268,435,456 particles), density 1, UDistribution::Thermal
+uth = 0.05 (the reference's own seeded generator), ufl = 0, FP32.  A step is
+one Simulation::advance (push + move/deposit + sort + current guard cells +
+Yee).  Metric: particle pushes per second (sum of particles moved per step,
+as Simulation::get_nmove counts them, divided by the step time).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (launched by torchrun) every rank runs its own replica of the
+workload (the path does not shard) and the timing is the
+maximum over ranks.  ``--impl reference`` times the reference's own OpenMP
+build (oracle/_ref, AVX2 variant) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, 'zpic-parallel_b200'), os.path.join(ROOT, 'oracle')):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+# workload (uniform warm plasma)
+NCELL = 2048
+TILE = 16
+PPC = 8
+UTH = 0.05
+DT = 0.07
+DX = 0.1
+METRIC = 'particle_pushes_per_second'
+UNIT = 'pushes/s'
+# algorithmic bytes (reference state layout): 56 B per particle push
+# (int2 cell + float2 position + float3 momentum, read and written); the
+# particle kernel also reads E and B (24 B/cell) and writes J (12 B/cell)
+BYTES_PER_PUSH = 56
+PARTICLE_KERNEL_BYTES_PER_CELL = 36
+
+
+def workload_config(ncell=NCELL):
+    return {
+        'workload': 'uniform warm plasma %dx%d cells, 16x16 tiles, 8x8 ppc, uth 0.05, periodic' % (ncell, ncell),
+        'cells': ncell * ncell, 'particles': ncell * ncell * PPC * PPC, 'tile': [TILE, TILE],
+        'dx': DX, 'dt': DT, 'species': 1,
+        'l2': 'inputs larger than L2 (particle state %.1f GB)' % (ncell * ncell * PPC * PPC * 24 / 1e9),
+    }
+
+
+def peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+def ncu_traffic_per_particle():
+    """DRAM bytes per particle of the particle kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, 'profiles', 'particles_uniform_plasma.md')
+    if not os.path.exists(p):
+        return None
+    m = re.search(r'dram_bytes_per_particle:\s*([0-9.]+)', open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.index),
+                 '--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+                 'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+                 'clocks_event_reasons.sw_power_cap',
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(',')]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[3 + k].lower() == 'active':
+                    reasons.add(name)
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': mx,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = 'nccl' if torch.cuda.is_available() else 'gloo'
+        if backend == 'nccl':
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = 'cuda' if torch.cuda.is_available() else 'cpu'
+    t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU reference arm: the reference's own OpenMP build (oracle/_ref)
+# ---------------------------------------------------------------------------
+def reference_sample(ncell, steps, warmup, threads=None):
+    from em2d_oracle import RefSim, ref_available
+    variant = 'avx2' if ref_available('avx2') else 'scalar'
+    nt = ncell // TILE
+    s = RefSim((nt, nt), (TILE, TILE), (ncell * DX, ncell * DX), DT, variant=variant,
+               threads=threads or os.cpu_count())
+    s.add_species(-1.0, (PPC, PPC), udist=('thermal', (UTH, UTH, UTH), (0, 0, 0)))
+    s.advance(warmup)
+    n0 = s.nmove()
+    t0 = time.perf_counter()
+    s.advance(steps)
+    dt = time.perf_counter() - t0
+    pushes = s.nmove() - n0
+    cores = s.threads
+    s.close()
+    return pushes / dt, dt / steps, cores, variant
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    from em2d_oracle import ref_available
+    if not ref_available('scalar') and not ref_available('avx2'):
+        print(json.dumps({'impl': 'reference', 'unavailable': 'reference build oracle/_ref missing'}))
+        return 0
+    # bounded sample of the workload: same tiles, ppc and temperature on a
+    # smaller box, so that the run finishes within a few minutes
+    ncell = args.ref_cells
+    rate, tstep, cores, variant = reference_sample(ncell, args.steps, args.warmup)
+    cfg = workload_config(NCELL)
+    line = {
+        'metric': METRIC, 'value': rate, 'unit': UNIT, 'impl': 'reference',
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': tstep * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded)',
+        'config': cfg,
+        'cpu_baseline': {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'reference',
+                         'sample': '%dx%d cells of the workload (%d particles), openmp/em2d %s build, '
+                                   '%d threads, step loop timed' % (ncell, ncell, ncell * ncell * PPC * PPC,
+                                                                    variant, cores)},
+        'e2e': {'value': rate, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def make_sim(zb, ncell, device):
+    nt = ncell // TILE
+    s = zb.Simulation((nt, nt), (TILE, TILE), (ncell * DX, ncell * DX), DT, device=device)
+    s.add_species(-1.0, (PPC, PPC), udist=('thermal', (UTH, UTH, UTH), (0, 0, 0)))
+    return s
+
+
+def run_gpu(args, world, rank, local):
+    import numpy as np
+    import torch
+    import zpic_b200 as zb
+
+    torch.cuda.set_device(local)
+    ncell = args.cells
+    sim = make_sim(zb, ncell, local)
+    np_total = sim.np_total(0)
+    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=local)
+
+    # warm-up (also captures the CUDA graph of one step)
+    sim.advance(args.warmup)
+    sim.synchronize()
+
+    # ---- device-timed region: K steps, inputs resident in HBM ----
+    l0 = sim.launch_count()
+    n0 = sim.nmove()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        sim.advance(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    t_ms = ev0.elapsed_time(ev1)
+    launches = sim.launch_count() - l0
+    pushes = sim.nmove() - n0
+    t_max = max_over_ranks(t_ms, world)
+    value = pushes * world / (t_max / 1e3)
+
+    # ---- per-kernel timing (CUDA events around each phase on the library stream) ----
+    sim.set_option('profile', 1)
+    sim.reset_phase_times()
+    sim.advance(args.steps)
+    sim.synchronize()
+    ph = sim.phase_times()
+    sim.set_option('profile', 0)
+    sim.set_option('graph', 1)
+    part_ms, part_n = ph['particles']
+    per_launch_ms = part_ms / max(1, part_n)
+    hbm, peak_kind = peaks()
+    alg_bytes = BYTES_PER_PUSH * np_total + PARTICLE_KERNEL_BYTES_PER_CELL * ncell * ncell
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    tpp = ncu_traffic_per_particle()
+    roofline = {
+        'kernel': 'k_particles (fused push, move, deposit, walls, leaver detection)',
+        'bound': 'hbm', 'achieved': achieved, 'peak': hbm, 'unit': 'GB/s',
+        'frac': achieved / hbm, 'peak_kind': peak_kind,
+        'traffic': (tpp * np_total) if tpp else None,
+        'algorithmic_bytes_per_launch': alg_bytes,
+        'launch_ms': per_launch_ms,
+        'phase_ms_per_step': {k: v[0] / args.steps for k, v in ph.items()},
+    }
+
+    # ---- end-to-end through the C-ABI with host buffers ----
+    # timed: upload of the particle state from pinned host memory, K steps,
+    # and the per-step energy diagnostics read back to the host (as
+    # Simulation::energy_info does)
+    npt, ix, x, u = sim.particles(0)
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    ix, x, u, npt = pin(ix), pin(x), pin(u), pin(npt)
+    h2d = ix.nbytes + x.nbytes + u.nbytes + npt.nbytes
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.set_particles(0, npt, ix, x, u)
+    for _ in range(args.steps):
+        sim.advance(1)
+        sim.species_energy(0)
+        sim.emf_energy()
+    sim.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = np_total * args.steps * world / e2e_s
+    # species energy (1 double) + per-tile field energy partials (6 doubles per
+    # tile, summed on the host in tile order as EMF::get_energy does)
+    d2h = 8 + 6 * 8 * (ncell // TILE) ** 2
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from em2d_oracle import ref_available
+            if ref_available('avx2') or ref_available('scalar'):
+                rate, tstep, cores, variant = reference_sample(args.ref_cells, args.ref_steps, 1)
+                cpu = {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'reference',
+                       'sample': '%dx%d cells of the workload (%d particles), openmp/em2d %s build, '
+                                 '%d steps, step loop timed' % (args.ref_cells, args.ref_cells,
+                                                                args.ref_cells ** 2 * PPC * PPC, variant,
+                                                                args.ref_steps)}
+        except Exception as e:  # reported, not fatal
+            cpu = {'value': None, 'error': str(e)}
+
+    clocks = clk.summary()
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': t_max / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded Thermal uth 0.05)',
+            'config': workload_config(ncell),
+            'roofline': roofline,
+            'cpu_baseline': cpu,
+            'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d / args.steps,
+                    'd2h_bytes_per_step': d2h,
+                    'note': 'particle state uploaded once from pinned host memory inside the timed '
+                            'region (bytes amortised over the K steps), energies read back every step'},
+            'gpu_launches': launches,
+            'clocks': clocks,
+            'cell_updates_per_second': ncell * ncell * args.steps * world / (t_max / 1e3),
+        }
+        print(json.dumps(line))
+    sim.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--cells', type=int, default=NCELL, help='grid size (cells per side)')
+    ap.add_argument('--ref-cells', type=int, default=512, help='CPU sample size (cells per side)')
+    ap.add_argument('--ref-steps', type=int, default=10)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == 'reference':
+            rc = run_reference(args, world, rank)
+        else:
+            rc = run_gpu(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -1,0 +1,221 @@
+"""Parity of the CUDA em2d step against the oracle (plain-C restatement of the
+reference openmp/em2d build), through the library's C-ABI.
+
+Bars (from the reference's arithmetic):
+* per-particle push and move, initial states, tile counts and per-tile
+  particle multisets: bit-exact;
+* the Yee solver and the current guard-cell sums on identical inputs: bit-exact;
+* deposited current: FP32 summation order differs (shared atomics vs the
+  reference's serial loop) -> max|dJ| <= 1e-6 * max|J|;
+* multi-step energy histories: relative agreement 1e-3 (chaotic growth of
+  round-off differences in an unstable plasma).
+"""
+import numpy as np
+import pytest
+
+from em2d_oracle import OracleSim
+import zpic_b200 as zb
+from helpers import same_multisets, interior_mask, rel_err, random_fields
+
+pytestmark = pytest.mark.gpu
+
+WEIBEL = ((8, 8), (16, 16), (12.8, 12.8), 0.07)
+J_TOL = 1e-6
+
+
+def weibel(sim):
+    sim.add_species(-1.0, (4, 4), udist=('thermalcorr', (0.1, 0.1, 0.1), (0, 0, 0.6)))
+    sim.add_species(1.0, (4, 4), udist=('thermalcorr', (0.1, 0.1, 0.1), (0, 0, -0.6)))
+    return sim
+
+
+def pair(setup, geom=WEIBEL):
+    return setup(OracleSim(*geom)), setup(zb.Simulation(*geom))
+
+
+def test_initial_state_bit_exact():
+    o, g = pair(weibel)
+    for sp in range(2):
+        a, b = o.particles(sp), g.particles(sp)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+def test_push_bit_exact():
+    o, g = pair(weibel)
+    E = random_fields(o, 1)
+    B = random_fields(o, 2)
+    for s in (o, g):
+        s.set_grid('E', E)
+        s.set_grid('B', B)
+    for sp in range(2):
+        o.species_push(sp)
+        g.species_push(sp)
+        a, b = o.particles(sp), g.particles(sp)
+        assert np.array_equal(a[3], b[3]), 'momenta differ'
+        assert abs(o.species_energy(sp) - g.species_energy(sp)) <= 1e-12 * abs(o.species_energy(sp))
+
+
+def test_euler_push_bit_exact():
+    geom = ((4, 4), (16, 16), (6.4, 6.4), 0.05)
+
+    def setup(s):
+        s.add_species(-1.0, (2, 2), udist=('thermal', (0.2, 0.1, 0.05), (0.1, 0, 0)), push_type=1)
+        return s
+    o, g = pair(setup, geom)
+    E, B = random_fields(o, 3, 2.0), random_fields(o, 4, 5.0)
+    for s in (o, g):
+        s.set_grid('E', E)
+        s.set_grid('B', B)
+    o.species_push(0)
+    g.species_push(0)
+    # sinf/cosf of the exact rotation come from different math libraries: allow 2 ulp
+    a, b = o.particles(0)[3], g.particles(0)[3]
+    assert np.allclose(a, b, rtol=3e-7, atol=1e-7)
+
+
+def test_move_deposit():
+    o, g = pair(weibel)
+    for s in (o, g):
+        s.current_zero()
+    for sp in range(2):
+        o.species_move(sp)
+        g.species_move(sp)
+        a, b = o.particles(sp), g.particles(sp)
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]), 'positions differ'
+    m = interior_mask(o)
+    assert rel_err(g.grid('J')[:, m], o.grid('J')[:, m]) <= J_TOL
+
+
+def test_tile_sort_multisets():
+    o, g = pair(weibel)
+    for s in (o, g):
+        s.current_zero()
+        for sp in range(2):
+            s.species_move(sp)
+        for sp in range(2):
+            s.species_tile_sort(sp)
+    for sp in range(2):
+        assert same_multisets(o.particles(sp), g.particles(sp))
+
+
+def test_current_advance_bit_exact():
+    o, g = pair(weibel)
+    rng = np.random.default_rng(5)
+    raw = rng.normal(size=(64, o.tile_vol, 3)).astype(np.float32)
+    for s in (o, g):
+        s.current_zero()
+        s.set_grid('J', raw)
+        s.current_advance()
+    m = interior_mask(o)
+    assert np.array_equal(o.grid('J')[:, m], g.grid('J')[:, m])
+
+
+def test_yee_bit_exact():
+    o, g = pair(weibel)
+    E, B, J = random_fields(o, 6), random_fields(o, 7), random_fields(o, 8)
+    for s in (o, g):
+        s.current_zero()
+        s.set_grid('J', J)
+        s.current_advance()
+        s.set_grid('E', E)
+        s.set_grid('B', B)
+        s.emf_advance(True)
+    m = interior_mask(o)
+    for w in 'EB':
+        assert np.array_equal(o.grid(w)[:, m], g.grid(w)[:, m]), w
+
+
+def test_one_step():
+    o, g = pair(weibel)
+    o.advance(1)
+    g.advance(1)
+    for sp in range(2):
+        assert same_multisets(o.particles(sp), g.particles(sp))
+        assert abs(o.species_energy(sp) - g.species_energy(sp)) <= 1e-12 * abs(o.species_energy(sp))
+    m = interior_mask(o)
+    assert rel_err(g.grid('J')[:, m], o.grid('J')[:, m]) <= J_TOL
+    # The field solve is bit-exact (test_yee_bit_exact), so after one step from
+    # E = B = 0 the field differences must be fully explained by the current's
+    # rounding differences: E = -dt J, B = -(dt/2) curl E twice.
+    dt, dx, dy = WEIBEL[3], WEIBEL[2][0] / 128, WEIBEL[2][1] / 128
+    eps = np.finfo(np.float32).eps
+    dJ = np.abs(g.grid('J')[:, m] - o.grid('J')[:, m]).max()
+    dE = np.abs(g.grid('E')[:, m] - o.grid('E')[:, m]).max()
+    dB = np.abs(g.grid('B')[:, m] - o.grid('B')[:, m]).max()
+    assert dE <= 1.1 * dt * dJ + 4 * eps * np.abs(o.grid('E')[:, m]).max()
+    assert dB <= 1.1 * dt * (1 / dx + 1 / dy) * dE + 4 * eps * np.abs(o.grid('B')[:, m]).max()
+    assert g.nmove() == o.nmove()
+
+
+def test_energy_history_weibel():
+    o, g = pair(weibel)
+    for _ in range(10):
+        o.advance(20)
+        g.advance(20)
+        for sp in range(2):
+            assert rel_err(g.species_energy(sp), o.species_energy(sp)) <= 1e-3
+        eo, bo = o.emf_energy()
+        eg, bg = g.emf_energy()
+        assert rel_err(eg.sum(), eo.sum()) <= 1e-3
+        assert rel_err(bg.sum(), bo.sum()) <= 1e-3
+    for sp in range(2):
+        assert np.array_equal(o.tiles(sp)[0].sum(), g.tiles(sp)[0].sum())
+
+
+def lwfa_small(s):
+    s.add_species(-1.0, (4, 2), density=('step', 1.0, 2.0, 0))
+    s.add_laser('gaussian', start=5.5, fwhm=1.0, a0=2.0, omega0=10.0, W0=1.5, focus=5.0, axis=3.2, sin_pol=1)
+    s.set_moving_window()
+    s.current_set_filter('compensated', 0, 2)
+    return s
+
+
+LWFA = ((16, 4), (16, 16), (256 * 0.025, 64 * 0.1), 0.022)
+
+
+def test_moving_window_laser():
+    o, g = pair(lwfa_small, LWFA)
+    m = interior_mask(o)
+    for w in 'EB':
+        assert np.array_equal(o.grid(w)[:, m], g.grid(w)[:, m]), 'laser fields ' + w
+    o.advance_mov_window(1)
+    g.advance_mov_window(1)
+    assert same_multisets(o.particles(0), g.particles(0))
+    for n in (30, 60):
+        o.advance_mov_window(n - o.iter())
+        g.advance_mov_window(n - g.iter())
+        assert np.array_equal(o.tiles(0)[0], g.tiles(0)[0]) or \
+            abs(int(o.tiles(0)[0].sum()) - int(g.tiles(0)[0].sum())) <= 2
+        eo, bo = o.emf_energy()
+        eg, bg = g.emf_energy()
+        assert rel_err(eg.sum(), eo.sum()) <= 1e-3
+        assert rel_err(bg.sum(), bo.sum()) <= 1e-3
+
+
+def walls(s):
+    s.add_species(-1.0, (2, 3), density=('slab', 1.0, 1.0, 5.0, 1),
+                  udist=('thermal', (0.2, 0.1, 0.05), (0.1, 0, 0)), bc=(2, 2, 2, 2))
+    s.add_species(2.0, (3, 2), density=('sphere', 0.5, 3.2, 3.2, 2.0),
+                  udist=('thermalcorr', (0.05, 0.2, 0.1), (0, 0.2, 0), 3), bc=(2, 2, 2, 2))
+    s.emf_set_bc((2, 3, 3, 2))
+    s.current_set_bc((2, 2, 2, 2))
+    s.current_set_filter('binomial', 1, 2)
+    s.add_laser('plane', start=3.0, fwhm=1.0, a0=1.0, omega0=5.0, polarization=0.3)
+    return s
+
+
+def test_walls_filters_profiles():
+    geom = ((4, 4), (16, 16), (6.4, 6.4), 0.05)
+    o, g = pair(walls, geom)
+    for sp in range(2):
+        assert same_multisets(o.particles(sp), g.particles(sp))
+    o.advance(1)
+    g.advance(1)
+    for sp in range(2):
+        assert same_multisets(o.particles(sp), g.particles(sp))
+    o.advance(40)
+    g.advance(40)
+    for sp in range(2):
+        assert o.tiles(sp)[0].sum() == g.tiles(sp)[0].sum()
+        assert rel_err(g.species_energy(sp), o.species_energy(sp)) <= 1e-3

@@ -1,0 +1,1448 @@
+// engine.cu -- host engine and C-ABI of libzpic_b200.so.
+//
+// A zpic_sim owns one simulation's device state (E, B, J, raw deposits,
+// species particle slots and sort scratch) and a CUDA stream.  Every step is
+// a fixed sequence of launches over work lists of (species, tile, chunk) and
+// (run, tile) items; a zpic_batch builds the same lists over many
+// simulations so that each phase of all of them is one launch.  Repeated
+// steps are captured once in a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "zpic_b200.h"
+#include "zpic_dev.cuh"
+#include "host_init.h"
+
+namespace zb {
+struct TileItem { int run; int tile; };
+struct InjRule {
+    int type; int diry; float a, b; float cx, cy, r2; float dxx, dxy; int ppcx, ppcy; int range[4]; int tx_limit;
+};
+size_t particle_smem_bytes( int tile_vol );
+cudaError_t launch_particles( cudaStream_t, int, int, int, const Item *, int, const SpDev *, const RunDev *, const int *, int );
+cudaError_t launch_sort( cudaStream_t, const Item *, int, const SpDev *, const int *, int, const RunDev *, int );
+cudaError_t launch_inject( cudaStream_t, int, int, const SpDev *, const RunDev *, const InjRule &, int );
+cudaError_t launch_pack( cudaStream_t, int, int, const SpDev *, const int *, int2 *, float2 *, float * );
+cudaError_t launch_unpack( cudaStream_t, int, int, const SpDev *, const int *, const int2 *, const float2 *, const float * );
+cudaError_t launch_gather( cudaStream_t, int, int, const SpDev *, const RunDev *, const int *, int, float, float, int, float * );
+cudaError_t launch_dep_charge( cudaStream_t, int, int, const SpDev *, const RunDev *, float *, int, int );
+cudaError_t launch_energy_sum( cudaStream_t, const SpDev *, int, int, double * );
+cudaError_t launch_np_stats( cudaStream_t, const SpDev *, int, unsigned long long * );
+cudaError_t launch_current_gc( cudaStream_t, const TileItem *, int, const RunDev * );
+cudaError_t launch_emf_gc( cudaStream_t, const TileItem *, int, const RunDev *, int );
+cudaError_t launch_cur_gc( cudaStream_t, const TileItem *, int, const RunDev *, int );
+cudaError_t launch_yee( cudaStream_t, const TileItem *, int, const RunDev *, int, int, int, int );
+cudaError_t launch_emf_bc( cudaStream_t, const RunDev *, int, int, int );
+cudaError_t launch_cur_bc( cudaStream_t, const RunDev *, int, int, int );
+cudaError_t launch_kernel3( cudaStream_t, const TileItem *, int, const RunDev *, int, int, float, float, float, int );
+cudaError_t launch_shift_left( cudaStream_t, const TileItem *, int, const RunDev *, int );
+cudaError_t launch_field_energy( cudaStream_t, const RunDev *, int, int, double * );
+cudaError_t launch_grid_add( cudaStream_t, float *, const float *, size_t );
+cudaError_t launch_charge_finish( cudaStream_t, const float *, float *, int, int, int, int, int, int, int, int );
+cudaError_t launch_grid_gather( cudaStream_t, const float *, float *, int, int, int, int, int, int, int, int );
+}  // namespace zb
+
+using namespace zb;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+static thread_local int g_device = -1;
+
+static int fail( int code, const std::string & msg ) { g_err = msg; return code; }
+
+#define CK( call )                                                                              \
+    do {                                                                                        \
+        cudaError_t e_ = ( call );                                                              \
+        if ( e_ != cudaSuccess )                                                                \
+            return fail( ZPIC_E_CUDA, std::string( #call ) + ": " + cudaGetErrorString( e_ ) ); \
+    } while ( 0 )
+
+#define TRY( call ) do { int r_ = ( call ); if ( r_ != ZPIC_OK ) return r_; } while ( 0 )
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+struct MovingWindow {          // moving_window.h:1-57
+    bool active = false; unsigned n_move = 0; double dx = 0;
+    void init( float d ) { active = true; n_move = 0; dx = d; }
+    void advance() { if ( active ) n_move++; }
+    double motion() const { return n_move * dx; }
+    bool needs_move( double t ) const { return active && ( t > dx * ( n_move + 1 ) ); }
+};
+
+template < class T > static int dalloc( T ** p, size_t n ) {
+    *p = nullptr;
+    if ( n == 0 ) n = 1;
+    cudaError_t e = cudaMalloc( (void **) p, n * sizeof( T ) );
+    if ( e != cudaSuccess ) return fail( ZPIC_E_NOMEM, std::string( "cudaMalloc: " ) + cudaGetErrorString( e ) );
+    return ZPIC_OK;
+}
+template < class T > static void dfree( T *& p ) { if ( p ) cudaFree( p ); p = nullptr; }
+
+static inline int roundup4( int n ) { return ( n + 3 ) & ~3; }
+
+enum Phase { PH_PARTICLES = 0, PH_SORT, PH_CURRENT, PH_FIELDS, PH_OTHER, PH_N };
+
+// ---------------------------------------------------------------------------
+// species
+// ---------------------------------------------------------------------------
+struct HSpecies {
+    std::string name;
+    float m_q = -1; uint32_t ppc[2] = { 1, 1 };
+    zpic_density dens{}; zpic_udist ud{};
+    int push_type = 0;
+    int bc[4] = { 1, 1, 1, 1 };
+    int id = 0;
+    float q = 0, dx[2] = { 0, 0 }, box[2] = { 0, 0 }, dt = 0;
+    int iter = 0;
+    MovingWindow mw;
+    int ntiles = 0;
+    uint32_t max_part = 0;
+    uint64_t np_bound = 0;    // upper bound of the particle count (capacity checks)
+    SpDev d{};                // descriptor (device pointers)
+    bool sort_pending = false;
+    bool counters_dirty = false;
+
+    void free_all() {
+        PartArrays * arrs[3] = { &d.A, &d.B, &d.S };
+        for ( auto * a : arrs ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
+        dfree( d.np ); dfree( d.off ); dfree( d.cap ); dfree( d.npt ); dfree( d.nidx ); dfree( d.idx );
+        dfree( d.aux ); dfree( d.aux2 ); dfree( d.in_cnt ); dfree( d.stage_off ); dfree( d.stage_cnt );
+        dfree( d.new_off ); dfree( d.new_cap ); dfree( d.new_np ); dfree( d.extra ); dfree( d.mode );
+        dfree( d.energy ); dfree( d.nmove );
+    }
+};
+
+static int alloc_arrays( PartArrays & a, size_t n ) {
+    TRY( dalloc( &a.cell, n ) ); TRY( dalloc( &a.xx, n ) ); TRY( dalloc( &a.xy, n ) );
+    TRY( dalloc( &a.ux, n ) ); TRY( dalloc( &a.uy, n ) ); TRY( dalloc( &a.uz, n ) );
+    return ZPIC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// plan: device work lists over a set of simulations
+// ---------------------------------------------------------------------------
+struct zpic_sim;
+
+struct Plan {
+    std::vector<zpic_sim *> sims;
+    RunDev * runs_d = nullptr;
+    SpDev * sps_d = nullptr;
+    std::vector<SpDev> sps_h;
+    std::vector<int> sp_sim, sp_local;          // plan species -> (sim index, species index)
+    Item * k1_items_d[2] = { nullptr, nullptr }; int n_k1[2] = { 0, 0 };   // boris, euler
+    Item * sort_items_d = nullptr; int n_sort = 0;
+    int * splist_d = nullptr; int n_sp = 0;
+    TileItem * tile_items_d = nullptr; int n_tiles = 0;
+    int max_tile_vol = 0;
+    bool needs_bc_or_filter = false;
+    cudaGraphExec_t graph = nullptr;
+    int graph_kernels = 0;
+    bool built = false;
+
+    void release() {
+        if ( graph ) { cudaGraphExecDestroy( graph ); graph = nullptr; }
+        dfree( runs_d ); dfree( sps_d ); dfree( k1_items_d[0] ); dfree( k1_items_d[1] );
+        dfree( sort_items_d ); dfree( splist_d ); dfree( tile_items_d );
+        built = false;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// simulation
+// ---------------------------------------------------------------------------
+struct zpic_sim {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int ntx, nty, nxx, nxy;
+    float box[2]; double dt;
+    float dx[2];
+    unsigned iter = 0;
+    // EMF (emf.h)
+    int emf_bc[4] = { 1, 1, 1, 1 };
+    int emf_iter = 0; MovingWindow emf_mw;
+    // Current (current.h)
+    int cur_bc[4] = { 1, 1, 1, 1 };
+    int cur_iter = 0; MovingWindow cur_mw;
+    int ftype = 0, fdir = 0; unsigned forder = 1;
+    bool j_final = false;          // J holds the summed current, else Jdep holds raw deposits
+    bool jdep_clean = true;
+    // device
+    RunDev run{};
+    int * status = nullptr;
+    double * dscratch = nullptr;   // small device scratch (energies, stats)
+    double * hscratch = nullptr;   // pinned host mirror
+    int * shifts_d = nullptr;
+    std::vector<HSpecies *> species;
+    Plan plan;
+    // options
+    bool use_graph = true;
+    int chunks_opt = 0;
+    bool profile = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[PH_N];
+    double phase_ms[PH_N] = { 0 };
+    uint64_t phase_launches[PH_N] = { 0 };
+    uint64_t launches = 0;
+
+    int tile_vol() const { return run.tile_vol; }
+    size_t grid_floats() const { return (size_t) run.tile_vol * ntx * nty * 3; }
+};
+
+struct zpic_batch {
+    std::vector<zpic_sim *> sims;
+    cudaStream_t stream = nullptr;
+    Plan plan;
+    cudaEvent_t ev = nullptr;
+};
+
+static int sim_select( zpic_sim * s ) {
+    if ( !s ) return fail( ZPIC_E_INVALID, "null simulation handle" );
+    CK( cudaSetDevice( s->device ) );
+    return ZPIC_OK;
+}
+
+static int check_status( zpic_sim * s ) {
+    int st = 0;
+    CK( cudaMemcpyAsync( &st, s->status, sizeof( int ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    if ( st & ( ST_WAIT_TIMEOUT | ST_CAPACITY | ST_BAD_CELL ) ) {
+        std::string m = "device reported:";
+        if ( st & ST_WAIT_TIMEOUT ) m += " bounded wait expired;";
+        if ( st & ST_CAPACITY ) m += " particle buffer capacity exceeded;";
+        if ( st & ST_BAD_CELL ) m += " particle moved more than one tile;";
+        return fail( ZPIC_E_DEVICE, m );
+    }
+    return ZPIC_OK;
+}
+
+// Chunks (CTAs) per tile for the particle kernel: enough work items to fill
+// the GPU a few times over (the reference splits tiles over blockIdx.z the
+// same way, cuda/em2d/species.cpp:924-937).
+static int auto_chunks( int ntiles_total, int opt ) {
+    if ( opt > 0 ) return opt;
+    int dev = 0; cudaGetDevice( &dev );
+    int sms = 148; cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
+    const int target = sms * 8;
+    if ( ntiles_total >= target ) return 1;
+    return std::min( 64, ( target + ntiles_total - 1 ) / ntiles_total );
+}
+
+static int upload_run( zpic_sim * s ) {
+    RunDev & R = s->run;
+    R.emf_perx = s->emf_bc[0] == ZPIC_EMF_BC_PERIODIC; R.emf_pery = s->emf_bc[2] == ZPIC_EMF_BC_PERIODIC;
+    R.cur_perx = s->cur_bc[0] == ZPIC_CURRENT_BC_PERIODIC; R.cur_pery = s->cur_bc[2] == ZPIC_CURRENT_BC_PERIODIC;
+    for ( int k = 0; k < 4; k++ ) { R.emf_bc[k] = s->emf_bc[k]; R.cur_bc[k] = s->cur_bc[k]; }
+    s->plan.built = false;
+    return ZPIC_OK;
+}
+
+// Build the work lists for a set of simulations (one sim, or a batch).
+static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims ) {
+    P.release();
+    P.sims = sims;
+    std::vector<RunDev> runs;
+    std::vector<Item> k1[2], sort_items;
+    std::vector<int> splist;
+    std::vector<TileItem> tiles;
+    P.sps_h.clear(); P.sp_sim.clear(); P.sp_local.clear();
+    P.max_tile_vol = 0;
+    P.needs_bc_or_filter = false;
+    int total_tiles = 0;
+    for ( auto * s : sims ) for ( auto * sp : s->species ) { (void) sp; total_tiles += s->ntx * s->nty; }
+    for ( size_t r = 0; r < sims.size(); r++ ) {
+        zpic_sim * s = sims[r];
+        runs.push_back( s->run );
+        P.max_tile_vol = std::max( P.max_tile_vol, s->run.tile_vol );
+        for ( int t = 0; t < s->ntx * s->nty; t++ ) tiles.push_back( { (int) r, t } );
+        for ( int k = 0; k < 4; k++ )
+            if ( s->emf_bc[k] > ZPIC_EMF_BC_PERIODIC || s->cur_bc[k] > ZPIC_CURRENT_BC_PERIODIC ) P.needs_bc_or_filter = true;
+        if ( s->ftype != ZPIC_FILTER_NONE || s->emf_mw.active ) P.needs_bc_or_filter = true;
+    }
+    for ( size_t r = 0; r < sims.size(); r++ ) {
+        zpic_sim * s = sims[r];
+        for ( size_t k = 0; k < s->species.size(); k++ ) {
+            HSpecies * sp = s->species[k];
+            SpDev d = sp->d;
+            d.run = (int) r;
+            const int gi = (int) P.sps_h.size();
+            P.sps_h.push_back( d );
+            P.sp_sim.push_back( (int) r ); P.sp_local.push_back( (int) k );
+            splist.push_back( gi );
+            for ( int t = 0; t < sp->ntiles; t++ ) {
+                for ( int c = 0; c < d.nchunk; c++ ) k1[ sp->push_type ? 1 : 0 ].push_back( { gi, t, c, 0 } );
+                sort_items.push_back( { gi, t, 0, 0 } );
+            }
+        }
+    }
+    P.n_sp = (int) splist.size();
+    TRY( dalloc( &P.runs_d, runs.size() ) );
+    TRY( dalloc( &P.sps_d, P.sps_h.size() ) );
+    TRY( dalloc( &P.splist_d, splist.size() ) );
+    TRY( dalloc( &P.tile_items_d, tiles.size() ) );
+    TRY( dalloc( &P.sort_items_d, sort_items.size() ) );
+    CK( cudaMemcpy( P.runs_d, runs.data(), runs.size() * sizeof( RunDev ), cudaMemcpyHostToDevice ) );
+    if ( !P.sps_h.empty() ) {
+        CK( cudaMemcpy( P.sps_d, P.sps_h.data(), P.sps_h.size() * sizeof( SpDev ), cudaMemcpyHostToDevice ) );
+        CK( cudaMemcpy( P.splist_d, splist.data(), splist.size() * sizeof( int ), cudaMemcpyHostToDevice ) );
+        CK( cudaMemcpy( P.sort_items_d, sort_items.data(), sort_items.size() * sizeof( Item ), cudaMemcpyHostToDevice ) );
+    }
+    CK( cudaMemcpy( P.tile_items_d, tiles.data(), tiles.size() * sizeof( TileItem ), cudaMemcpyHostToDevice ) );
+    for ( int p = 0; p < 2; p++ ) {
+        P.n_k1[p] = (int) k1[p].size();
+        TRY( dalloc( &P.k1_items_d[p], k1[p].size() ) );
+        if ( !k1[p].empty() )
+            CK( cudaMemcpy( P.k1_items_d[p], k1[p].data(), k1[p].size() * sizeof( Item ), cudaMemcpyHostToDevice ) );
+    }
+    P.n_sort = (int) sort_items.size();
+    P.n_tiles = (int) tiles.size();
+    P.built = true;
+    return ZPIC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// profiling helpers
+// ---------------------------------------------------------------------------
+struct PhaseScope {
+    zpic_sim * s; cudaStream_t st; int ph; cudaEvent_t a = nullptr, b = nullptr; int nl;
+    PhaseScope( zpic_sim * s_, cudaStream_t st_, int ph_, int nlaunch ) : s( s_ ), st( st_ ), ph( ph_ ), nl( nlaunch ) {
+        if ( s && s->profile ) { cudaEventCreate( &a ); cudaEventCreate( &b ); cudaEventRecord( a, st ); }
+    }
+    ~PhaseScope() {
+        if ( !s ) return;
+        s->launches += nl;
+        s->phase_launches[ph] += nl;
+        if ( s->profile ) { cudaEventRecord( b, st ); s->ev_pending[ph].push_back( { a, b } ); }
+    }
+};
+
+static void resolve_phase_events( zpic_sim * s ) {
+    for ( int p = 0; p < PH_N; p++ ) {
+        for ( auto & e : s->ev_pending[p] ) {
+            float ms = 0;
+            cudaEventSynchronize( e.second );
+            cudaEventElapsedTime( &ms, e.first, e.second );
+            s->phase_ms[p] += ms;
+            cudaEventDestroy( e.first ); cudaEventDestroy( e.second );
+        }
+        s->ev_pending[p].clear();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// step pieces
+// ---------------------------------------------------------------------------
+static zpic_sim * prof_sim( Plan & P ) { return P.sims.size() == 1 ? P.sims[0] : nullptr; }
+
+// push + move + deposit + walls + leaver detection for all species of the plan
+static int run_particles( Plan & P, cudaStream_t st, int push, int move, const int * shifts ) {
+    for ( int p = 0; p < 2; p++ ) {
+        if ( P.n_k1[p] == 0 ) continue;
+        PhaseScope ps( prof_sim( P ), st, PH_PARTICLES, 1 );
+        CK( launch_particles( st, push ? p + 1 : 0, move, 1, P.k1_items_d[p], P.n_k1[p], P.sps_d, P.runs_d, shifts, P.max_tile_vol ) );
+    }
+    return ZPIC_OK;
+}
+
+static int run_sort( Plan & P, cudaStream_t st, int use_extra ) {
+    if ( P.n_sp == 0 ) return ZPIC_OK;
+    PhaseScope ps( prof_sim( P ), st, PH_SORT, 3 );
+    CK( launch_sort( st, P.sort_items_d, P.n_sort, P.sps_d, P.splist_d, P.n_sp, P.runs_d, use_extra ) );
+    return ZPIC_OK;
+}
+
+// Current::advance device part for every run of the plan (current.cpp:227-246)
+static int run_current( Plan & P, cudaStream_t st ) {
+    {
+        PhaseScope ps( prof_sim( P ), st, PH_CURRENT, 1 );
+        CK( launch_current_gc( st, P.tile_items_d, P.n_tiles, P.runs_d ) );
+    }
+    if ( !P.needs_bc_or_filter ) return ZPIC_OK;
+    for ( size_t r = 0; r < P.sims.size(); r++ ) {
+        zpic_sim * s = P.sims[r];
+        if ( s->cur_bc[0] > 1 || s->cur_bc[1] > 1 ) {
+            PhaseScope ps( prof_sim( P ), st, PH_CURRENT, 1 );
+            CK( launch_cur_bc( st, P.runs_d, (int) r, 0, 2 * s->nty * s->run.exty ) );
+        }
+        if ( s->cur_bc[2] > 1 || s->cur_bc[3] > 1 ) {
+            PhaseScope ps( prof_sim( P ), st, PH_CURRENT, 1 );
+            CK( launch_cur_bc( st, P.runs_d, (int) r, 1, 2 * s->ntx * s->run.extx ) );
+        }
+    }
+    // filters (filter.h:22-86): run-specific, launched over all tiles of the plan only when uniform
+    for ( size_t r = 0; r < P.sims.size(); r++ ) {
+        zpic_sim * s = P.sims[r];
+        if ( s->ftype == ZPIC_FILTER_NONE ) continue;
+        const unsigned order = s->forder > 0 ? s->forder : 1;
+        // tile items of this run only
+        int first = 0;
+        for ( size_t q = 0; q < r; q++ ) first += P.sims[q]->ntx * P.sims[q]->nty;
+        const int nt = s->ntx * s->nty;
+        const TileItem * items = P.tile_items_d + first;
+        auto pass = [&]( float a, float b, float c ) -> int {
+            PhaseScope ps( prof_sim( P ), st, PH_CURRENT, 2 );
+            CK( launch_kernel3( st, items, nt, P.runs_d, 2, s->fdir, a, b, c, P.max_tile_vol ) );
+            CK( launch_cur_gc( st, items, nt, P.runs_d, s->fdir ? 2 : 1 ) );
+            return ZPIC_OK;
+        };
+        for ( unsigned i = 0; i < order; i++ ) TRY( pass( 0.25f, 0.5f, 0.25f ) );
+        if ( s->ftype == ZPIC_FILTER_COMPENSATED ) {
+            const float a = -1.0f;
+            const float b = ( 4.0 + 2.0 * order ) / order;
+            const float norm = 2 * a + b;
+            TRY( pass( a / norm, b / norm, a / norm ) );
+        }
+    }
+    return ZPIC_OK;
+}
+
+// EMF::advance device part (emf.cpp:513-580 and 135-194): Yee, guard cells, bc
+static int run_fields( Plan & P, cudaStream_t st, int with_j, int j_raw, int clear_jdep ) {
+    {
+        PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 2 );
+        CK( launch_yee( st, P.tile_items_d, P.n_tiles, P.runs_d, with_j, j_raw, clear_jdep, P.max_tile_vol ) );
+        CK( launch_emf_gc( st, P.tile_items_d, P.n_tiles, P.runs_d, 3 ) );
+    }
+    if ( !P.needs_bc_or_filter ) return ZPIC_OK;
+    for ( size_t r = 0; r < P.sims.size(); r++ ) {
+        zpic_sim * s = P.sims[r];
+        if ( s->emf_bc[0] > 1 || s->emf_bc[1] > 1 ) {
+            PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 1 );
+            CK( launch_emf_bc( st, P.runs_d, (int) r, 0, 2 * s->nty * s->run.exty ) );
+        }
+        if ( s->emf_bc[2] > 1 || s->emf_bc[3] > 1 ) {
+            PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 1 );
+            CK( launch_emf_bc( st, P.runs_d, (int) r, 1, 2 * s->ntx * s->run.extx ) );
+        }
+    }
+    return ZPIC_OK;
+}
+
+// EMF::move_window (emf.cpp:120-129) for one run of the plan
+static int run_shift( Plan & P, cudaStream_t st, int r ) {
+    int first = 0;
+    for ( int q = 0; q < r; q++ ) first += P.sims[q]->ntx * P.sims[q]->nty;
+    const int nt = P.sims[r]->ntx * P.sims[r]->nty;
+    PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 2 );
+    CK( launch_shift_left( st, P.tile_items_d + first, nt, P.runs_d, P.max_tile_vol ) );
+    CK( launch_emf_gc( st, P.tile_items_d + first, nt, P.runs_d, 1 ) );
+    return ZPIC_OK;
+}
+
+static int ensure_plan( zpic_sim * s ) {
+    if ( !s->plan.built ) TRY( plan_build( s->plan, { s } ) );
+    return ZPIC_OK;
+}
+
+static int ensure_jdep_clean( zpic_sim * s, cudaStream_t st ) {
+    if ( !s->jdep_clean ) {
+        CK( cudaMemsetAsync( s->run.Jdep, 0, s->grid_floats() * sizeof( float ), st ) );
+        s->jdep_clean = true;
+    }
+    return ZPIC_OK;
+}
+
+// One Simulation::advance (simulation.h:90-107) for all sims of a plan, on st.
+static int plan_step_device( Plan & P, cudaStream_t st ) {
+    TRY( run_particles( P, st, 1, 2, nullptr ) );
+    TRY( run_sort( P, st, 0 ) );
+    TRY( run_current( P, st ) );
+    TRY( run_fields( P, st, 1, 0, 1 ) );
+    return ZPIC_OK;
+}
+
+static void plan_step_host( Plan & P ) {
+    for ( auto * s : P.sims ) {
+        for ( auto * sp : s->species ) { sp->iter++; sp->sort_pending = false; sp->counters_dirty = false; }
+        s->cur_iter++;
+        if ( s->cur_mw.needs_move( s->cur_iter * s->dt ) ) s->cur_mw.advance();
+        s->emf_iter++;
+        s->j_final = true;
+        s->jdep_clean = true;
+        s->iter++;
+    }
+}
+
+static int count_graph_kernels( cudaGraph_t g ) {
+    size_t n = 0;
+    cudaGraphGetNodes( g, nullptr, &n );
+    std::vector<cudaGraphNode_t> nodes( n );
+    cudaGraphGetNodes( g, nodes.data(), &n );
+    int k = 0;
+    for ( auto & nd : nodes ) { cudaGraphNodeType t; cudaGraphNodeGetType( nd, &t ); if ( t == cudaGraphNodeTypeKernel ) k++; }
+    return k;
+}
+
+static int plan_advance( Plan & P, cudaStream_t st, int nsteps, bool use_graph, uint64_t * launches ) {
+    for ( auto * s : P.sims ) TRY( ensure_jdep_clean( s, st ) );
+    const bool can_graph = use_graph && nsteps > 1;
+    if ( can_graph && !P.graph ) {
+        // Capture one step.  Launch counting and profiling are suspended
+        // during capture; replays count the graph's kernel nodes instead.
+        std::vector<uint64_t> l0;
+        std::vector<char> prof;
+        for ( auto * s : P.sims ) { l0.push_back( s->launches ); prof.push_back( s->profile ); s->profile = false; }
+        cudaGraph_t g;
+        CK( cudaStreamBeginCapture( st, cudaStreamCaptureModeThreadLocal ) );
+        const int rc = plan_step_device( P, st );
+        const cudaError_t e = cudaStreamEndCapture( st, &g );
+        for ( size_t i = 0; i < P.sims.size(); i++ ) { P.sims[i]->launches = l0[i]; P.sims[i]->profile = prof[i]; }
+        if ( rc != ZPIC_OK ) return rc;
+        if ( e != cudaSuccess ) return fail( ZPIC_E_CUDA, std::string( "graph capture: " ) + cudaGetErrorString( e ) );
+        P.graph_kernels = count_graph_kernels( g );
+        const cudaError_t e2 = cudaGraphInstantiate( &P.graph, g, 0 );
+        cudaGraphDestroy( g );
+        if ( e2 != cudaSuccess ) { P.graph = nullptr; return fail( ZPIC_E_CUDA, std::string( "graph instantiate: " ) + cudaGetErrorString( e2 ) ); }
+    }
+    for ( int n = 0; n < nsteps; n++ ) {
+        if ( can_graph && P.graph ) {
+            CK( cudaGraphLaunch( P.graph, st ) );
+            if ( launches ) *launches += P.graph_kernels;
+        } else {
+            TRY( plan_step_device( P, st ) );
+        }
+        plan_step_host( P );
+    }
+    return ZPIC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// species set-up
+// ---------------------------------------------------------------------------
+
+// Slot layout: need[t] = roundup4(np[t] + extra[t]); free capacity spread in
+// proportion to need + min_slack (multiples of 4).
+static void slot_layout( const std::vector<int> & np, uint64_t max_part, int min_slack,
+                         std::vector<int> & off, std::vector<int> & cap ) {
+    const int nt = (int) np.size();
+    off.assign( nt, 0 ); cap.assign( nt, 0 );
+    long long need_sum = 0, w_sum = 0;
+    for ( int t = 0; t < nt; t++ ) { const int nd = roundup4( np[t] ); need_sum += nd; w_sum += nd + min_slack; }
+    const long long free_cap = std::max<long long>( 0, (long long) max_part - need_sum );
+    long long o = 0;
+    for ( int t = 0; t < nt; t++ ) {
+        const int nd = roundup4( np[t] );
+        const long long sl = w_sum > 0 ? ( free_cap * ( nd + min_slack ) ) / w_sum : 0;
+        cap[t] = nd + (int) ( sl & ~3LL );
+        off[t] = (int) o;
+        o += cap[t];
+    }
+}
+
+// Upload packed particles (reference layout) into the slot layout of sp.
+static int species_upload( zpic_sim * s, HSpecies * sp, const std::vector<int> & np,
+                           const int32_t * ix, const float * x, const float * u ) {
+    const int nt = sp->ntiles;
+    std::vector<int> poff( nt ); long long total = 0;
+    for ( int t = 0; t < nt; t++ ) { poff[t] = (int) total; total += np[t]; }
+    std::vector<int> off, cap;
+    const int min_slack = std::max<int>( 16, (int) ( sp->ppc[0] * sp->ppc[1] * s->nxx * s->nxy / 8 ) );
+    slot_layout( np, sp->max_part, min_slack, off, cap );
+    if ( (long long) off.back() + cap.back() > (long long) sp->max_part || [&] {
+             for ( int t = 0; t < nt; t++ ) if ( cap[t] < np[t] ) return true; return false; }() )
+        return fail( ZPIC_E_NOMEM, "particle set does not fit the species buffer" );
+    cudaStream_t st = s->stream;
+    CK( cudaMemcpyAsync( sp->d.np, np.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
+    CK( cudaMemcpyAsync( sp->d.off, off.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
+    CK( cudaMemcpyAsync( sp->d.cap, cap.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
+    int * poff_d = nullptr; int2 * ix_d = nullptr; float2 * x_d = nullptr; float * u_d = nullptr;
+    TRY( dalloc( &poff_d, nt ) );
+    TRY( dalloc( &ix_d, total ) ); TRY( dalloc( &x_d, total ) ); TRY( dalloc( &u_d, 3 * total ) );
+    CK( cudaMemcpyAsync( poff_d, poff.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
+    if ( total > 0 ) {
+        CK( cudaMemcpyAsync( ix_d, ix, total * sizeof( int2 ), cudaMemcpyHostToDevice, st ) );
+        CK( cudaMemcpyAsync( x_d, x, total * sizeof( float2 ), cudaMemcpyHostToDevice, st ) );
+        CK( cudaMemcpyAsync( u_d, u, total * 3 * sizeof( float ), cudaMemcpyHostToDevice, st ) );
+    }
+    // the species descriptor must be on the device for the unpack kernel
+    SpDev * one = nullptr;
+    TRY( dalloc( &one, 1 ) );
+    CK( cudaMemcpyAsync( one, &sp->d, sizeof( SpDev ), cudaMemcpyHostToDevice, st ) );
+    CK( launch_unpack( st, 0, nt, one, poff_d, ix_d, x_d, u_d ) );
+    s->launches++;
+    CK( cudaMemsetAsync( sp->d.npt, 0, 9 * nt * sizeof( int ), st ) );
+    CK( cudaMemsetAsync( sp->d.nidx, 0, nt * sizeof( int ), st ) );
+    CK( cudaStreamSynchronize( st ) );
+    dfree( one ); dfree( poff_d ); dfree( ix_d ); dfree( x_d ); dfree( u_d );
+    sp->np_bound = total;
+    sp->sort_pending = false;
+    sp->counters_dirty = false;
+    return ZPIC_OK;
+}
+
+static int species_alloc( zpic_sim * s, HSpecies * sp, uint64_t max_part ) {
+    const int nt = s->ntx * s->nty;
+    sp->ntiles = nt;
+    sp->max_part = (uint32_t) max_part;
+    SpDev & d = sp->d;
+    d.ntiles = nt;
+    d.max_part = (int) max_part;
+    d.stage_cap = (int) std::max<uint64_t>( 65536, max_part / 4 );
+    TRY( alloc_arrays( d.A, max_part ) );
+    TRY( alloc_arrays( d.B, max_part ) );
+    TRY( alloc_arrays( d.S, d.stage_cap ) );
+    TRY( dalloc( &d.np, nt ) ); TRY( dalloc( &d.off, nt ) ); TRY( dalloc( &d.cap, nt ) );
+    TRY( dalloc( &d.npt, 9 * nt ) ); TRY( dalloc( &d.nidx, nt ) );
+    TRY( dalloc( &d.idx, max_part ) ); TRY( dalloc( &d.aux, max_part ) ); TRY( dalloc( &d.aux2, max_part ) );
+    TRY( dalloc( &d.in_cnt, nt ) ); TRY( dalloc( &d.stage_off, nt ) ); TRY( dalloc( &d.stage_cnt, nt ) );
+    TRY( dalloc( &d.new_off, nt ) ); TRY( dalloc( &d.new_cap, nt ) ); TRY( dalloc( &d.new_np, nt ) );
+    TRY( dalloc( &d.extra, nt ) ); TRY( dalloc( &d.mode, 1 ) );
+    TRY( dalloc( &d.nmove, 1 ) );
+    CK( cudaMemset( d.nmove, 0, sizeof( unsigned long long ) ) );
+    CK( cudaMemset( d.extra, 0, nt * sizeof( int ) ) );
+    CK( cudaMemset( d.mode, 0, sizeof( int ) ) );
+    return ZPIC_OK;
+}
+
+static void species_params( zpic_sim * s, HSpecies * sp ) {
+    SpDev & d = sp->d;
+    d.alpha = 0.5 * sp->dt / sp->m_q;                  // species.cpp:2305
+    d.dt_dx = sp->dt / sp->dx[0]; d.dt_dy = sp->dt / sp->dx[1];
+    d.q = sp->q;
+    d.qnx = sp->q * sp->dx[0] / sp->dt; d.qny = sp->q * sp->dx[1] / sp->dt;
+    d.perx = sp->bc[0] == ZPIC_SPECIES_BC_PERIODIC;
+    d.pery = sp->bc[2] == ZPIC_SPECIES_BC_PERIODIC;
+    for ( int k = 0; k < 4; k++ ) d.bc[k] = sp->bc[k];
+    d.min_slack = std::max<int>( 16, (int) ( sp->ppc[0] * sp->ppc[1] * s->nxx * s->nxy / 8 ) );
+    d.run = 0;
+}
+
+static zbhost::TileGeom geom( zpic_sim * s ) { return { s->ntx, s->nty, s->nxx, s->nxy }; }
+
+static zbhost::Injector injector( zpic_sim * s, HSpecies * sp ) {
+    zbhost::Injector I;
+    I.dens = sp->dens;
+    I.ppc[0] = sp->ppc[0]; I.ppc[1] = sp->ppc[1];
+    I.dx[0] = sp->dx[0]; I.dx[1] = sp->dx[1];
+    I.motion = sp->mw.motion();
+    I.g = geom( s );
+    return I;
+}
+
+static InjRule inj_rule( zpic_sim * s, HSpecies * sp, const unsigned range[4] ) {
+    zbhost::Injector I = injector( s, sp );
+    InjRule r{};
+    r.type = sp->dens.type; r.diry = sp->dens.dir != 0;
+    I.rule_params( r.a, r.b, r.cx, r.cy, r.r2 );
+    r.dxx = sp->dx[0]; r.dxy = sp->dx[1];
+    r.ppcx = sp->ppc[0]; r.ppcy = sp->ppc[1];
+    for ( int k = 0; k < 4; k++ ) r.range[k] = range[k];
+    r.tx_limit = I.tx_limit();
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// species advance pieces (single simulation)
+// ---------------------------------------------------------------------------
+static int species_index( zpic_sim * s, int sp ) {
+    if ( sp < 0 || sp >= (int) s->species.size() ) return fail( ZPIC_E_INVALID, "invalid species index" );
+    return ZPIC_OK;
+}
+
+// plan-level species index of local species sp in a single-sim plan
+static int plan_sp( zpic_sim * s, int sp ) { (void) s; return sp; }
+
+// Launch the particle kernel for one species of a single simulation.
+static int species_kernel( zpic_sim * s, int sp, int push, int move, const int * shifts ) {
+    TRY( ensure_plan( s ) );
+    HSpecies * h = s->species[sp];
+    if ( h->counters_dirty && move ) {
+        CK( cudaMemsetAsync( h->d.npt, 0, 9 * h->ntiles * sizeof( int ), s->stream ) );
+        CK( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
+    }
+    // items of this species: rebuild a small list (per-species launches are the fine-grained API path)
+    std::vector<Item> items;
+    for ( int t = 0; t < h->ntiles; t++ ) for ( int c = 0; c < h->d.nchunk; c++ ) items.push_back( { plan_sp( s, sp ), t, c, 0 } );
+    Item * items_d = nullptr;
+    TRY( dalloc( &items_d, items.size() ) );
+    CK( cudaMemcpyAsync( items_d, items.data(), items.size() * sizeof( Item ), cudaMemcpyHostToDevice, s->stream ) );
+    {
+        PhaseScope ps( s, s->stream, PH_PARTICLES, 1 );
+        CK( launch_particles( s->stream, push ? 1 + h->push_type : 0, move, move ? 1 : 0, items_d, (int) items.size(),
+                              s->plan.sps_d, s->plan.runs_d, shifts, s->plan.max_tile_vol ) );
+    }
+    CK( cudaStreamSynchronize( s->stream ) );
+    dfree( items_d );
+    if ( move ) { h->sort_pending = true; h->counters_dirty = true; }
+    if ( move == 2 ) s->jdep_clean = false;
+    return ZPIC_OK;
+}
+
+static int species_sort( zpic_sim * s, int sp, int use_extra ) {
+    TRY( ensure_plan( s ) );
+    HSpecies * h = s->species[sp];
+    if ( !h->sort_pending ) {
+        // leaver lists are stale: detect them now (bnd_check, particles.cpp:212-303)
+        CK( cudaMemsetAsync( h->d.npt, 0, 9 * h->ntiles * sizeof( int ), s->stream ) );
+        CK( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
+        std::vector<Item> items;
+        for ( int t = 0; t < h->ntiles; t++ ) items.push_back( { sp, t, 0, 0 } );
+        Item * items_d = nullptr;
+        TRY( dalloc( &items_d, items.size() ) );
+        CK( cudaMemcpyAsync( items_d, items.data(), items.size() * sizeof( Item ), cudaMemcpyHostToDevice, s->stream ) );
+        {
+            PhaseScope ps( s, s->stream, PH_SORT, 1 );
+            CK( launch_particles( s->stream, 0, 0, 1, items_d, (int) items.size(), s->plan.sps_d, s->plan.runs_d, nullptr, s->plan.max_tile_vol ) );
+        }
+        CK( cudaStreamSynchronize( s->stream ) );
+        dfree( items_d );
+    }
+    std::vector<Item> items;
+    for ( int t = 0; t < h->ntiles; t++ ) items.push_back( { sp, t, 0, 0 } );
+    Item * items_d = nullptr; int * list_d = nullptr;
+    TRY( dalloc( &items_d, items.size() ) ); TRY( dalloc( &list_d, 1 ) );
+    CK( cudaMemcpyAsync( items_d, items.data(), items.size() * sizeof( Item ), cudaMemcpyHostToDevice, s->stream ) );
+    CK( cudaMemcpyAsync( list_d, &sp, sizeof( int ), cudaMemcpyHostToDevice, s->stream ) );
+    {
+        PhaseScope ps( s, s->stream, PH_SORT, 3 );
+        CK( launch_sort( s->stream, items_d, (int) items.size(), s->plan.sps_d, list_d, 1, s->plan.runs_d, use_extra ) );
+    }
+    CK( cudaStreamSynchronize( s->stream ) );
+    dfree( items_d ); dfree( list_d );
+    h->sort_pending = false;
+    h->counters_dirty = false;
+    return check_status( s );
+}
+
+// Species::advance_mov_window (species.cpp:2083-2128) for one species
+static int species_advance_mw( zpic_sim * s, int sp ) {
+    HSpecies * h = s->species[sp];
+    TRY( ensure_plan( s ) );
+    const float t = ( h->iter + 1 ) * h->dt;        // int * float, as in the reference
+    if ( h->mw.needs_move( t ) ) {
+        std::vector<int> shifts( s->species.size(), 0 );
+        shifts[sp] = -1;
+        CK( cudaMemcpyAsync( s->shifts_d, shifts.data(), shifts.size() * sizeof( int ), cudaMemcpyHostToDevice, s->stream ) );
+        TRY( species_kernel( s, sp, 1, 2, s->shifts_d ) );
+        const unsigned gx = s->ntx * s->nxx, gy = s->nty * s->nxy;
+        const unsigned range[4] = { gx - 1, gx - 1, 0, gy - 1 };
+        InjRule r = inj_rule( s, h, range );
+        // host-side bound of the particle count (exact injection count)
+        std::vector<int> extra( h->ntiles, 0 );
+        injector( s, h ).count( range, extra.data() );
+        uint64_t add = 0; for ( int v : extra ) add += v;
+        h->np_bound += add;
+        if ( h->np_bound > h->max_part ) {
+            // the bound is loose once particles leave; read the real count
+            unsigned long long st2[2];
+            CK( launch_np_stats( s->stream, s->plan.sps_d, sp, (unsigned long long *) s->dscratch ) );
+            CK( cudaMemcpyAsync( st2, s->dscratch, sizeof( st2 ), cudaMemcpyDeviceToHost, s->stream ) );
+            CK( cudaStreamSynchronize( s->stream ) );
+            h->np_bound = st2[0] + add;
+            if ( h->np_bound > h->max_part ) return fail( ZPIC_E_NOMEM, "particle buffer too small for the moving-window injection" );
+        }
+        if ( h->dens.type != ZPIC_DENSITY_NONE ) {
+            CK( launch_inject( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, r, 1 ) );
+            s->launches++;
+        }
+        TRY( species_sort( s, sp, h->dens.type != ZPIC_DENSITY_NONE ) );
+        if ( h->dens.type != ZPIC_DENSITY_NONE ) {
+            CK( launch_inject( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, r, 0 ) );
+            s->launches++;
+        }
+        h->mw.advance();
+    } else {
+        TRY( species_kernel( s, sp, 1, 2, nullptr ) );
+        TRY( species_sort( s, sp, 0 ) );
+    }
+    h->iter++;
+    return ZPIC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char * zpic_b200_last_error( void ) { return g_err.c_str(); }
+int zpic_b200_version( void ) { return 10000; }
+
+int zpic_b200_set_device( int device ) {
+    int n = 0;
+    CK( cudaGetDeviceCount( &n ) );
+    if ( device < 0 || device >= n ) return fail( ZPIC_E_INVALID, "invalid device" );
+    g_device = device;
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_create( uint32_t ntx, uint32_t nty, uint32_t nxx, uint32_t nxy,
+                          float boxx, float boxy, double dt, zpic_sim ** out ) {
+    if ( !out ) return fail( ZPIC_E_INVALID, "null output" );
+    *out = nullptr;
+    if ( ntx == 0 || nty == 0 ) return fail( ZPIC_E_INVALID, "Invalid number of tiles" );      // grid.h:34-38
+    if ( nxx == 0 || nxy == 0 ) return fail( ZPIC_E_INVALID, "Invalid tile size" );            // grid.h:40-43
+    if ( nxx > 4096 || nxy > 4096 ) return fail( ZPIC_E_INVALID, "tile size above 4096 cells" );
+    // Courant condition (emf.cpp:20-28)
+    const float dxx = boxx / ( nxx * ntx ), dxy = boxy / ( nxy * nty );
+    const float cour = std::sqrt( 1.0f / ( 1.0f / ( dxx * dxx ) + 1.0f / ( dxy * dxy ) ) );
+    if ( dt >= cour ) {
+        char m[160];
+        snprintf( m, sizeof m, "Invalid timestep, courant condition violation: the maximum timestep is dt = %g", cour );
+        return fail( ZPIC_E_INVALID, m );
+    }
+    int dev = g_device;
+    if ( dev < 0 ) CK( cudaGetDevice( &dev ) );
+    CK( cudaSetDevice( dev ) );
+    auto s = std::make_unique<zpic_sim>();
+    s->device = dev;
+    s->ntx = ntx; s->nty = nty; s->nxx = nxx; s->nxy = nxy;
+    s->box[0] = boxx; s->box[1] = boxy; s->dt = dt;
+    s->dx[0] = dxx; s->dx[1] = dxy;
+    CK( cudaStreamCreateWithFlags( &s->stream, cudaStreamNonBlocking ) );
+    RunDev & R = s->run;
+    R.ntx = ntx; R.nty = nty; R.nxx = nxx; R.nxy = nxy;
+    R.extx = 1 + nxx + 2; R.exty = 1 + nxy + 2;
+    R.gc_off = 1 * R.extx + 1;
+    R.tile_vol = roundup4( R.extx * R.exty );
+    const float dtx = dt / dxx, dty = dt / dxy;                 // emf.cpp:524-525
+    R.dtx = dtx; R.dty = dty; R.dtx2 = dtx / 2; R.dty2 = dty / 2;
+    R.dt = (float) dt;
+    const size_t nf = s->grid_floats();
+    TRY( dalloc( &R.E, nf ) ); TRY( dalloc( &R.B, nf ) ); TRY( dalloc( &R.J, nf ) ); TRY( dalloc( &R.Jdep, nf ) );
+    CK( cudaMemset( R.E, 0, nf * sizeof( float ) ) );
+    CK( cudaMemset( R.B, 0, nf * sizeof( float ) ) );
+    CK( cudaMemset( R.J, 0, nf * sizeof( float ) ) );
+    CK( cudaMemset( R.Jdep, 0, nf * sizeof( float ) ) );
+    TRY( dalloc( &s->status, 1 ) );
+    CK( cudaMemset( s->status, 0, sizeof( int ) ) );
+    R.status = s->status;
+    TRY( dalloc( &s->dscratch, 64 ) );
+    CK( cudaMallocHost( (void **) &s->hscratch, 64 * sizeof( double ) ) );
+    TRY( dalloc( &s->shifts_d, 64 ) );
+    TRY( upload_run( s.get() ) );
+    *out = s.release();
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_destroy( zpic_sim * s ) {
+    if ( !s ) return ZPIC_OK;
+    cudaSetDevice( s->device );
+    cudaStreamSynchronize( s->stream );
+    resolve_phase_events( s );
+    s->plan.release();
+    for ( auto * sp : s->species ) { sp->free_all(); delete sp; }
+    dfree( s->run.E ); dfree( s->run.B ); dfree( s->run.J ); dfree( s->run.Jdep );
+    dfree( s->status ); dfree( s->dscratch ); dfree( s->shifts_d );
+    if ( s->hscratch ) cudaFreeHost( s->hscratch );
+    cudaStreamDestroy( s->stream );
+    delete s;
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_add_species( zpic_sim * s, const zpic_species_desc * desc, int32_t * species_id ) {
+    TRY( sim_select( s ) );
+    if ( !desc ) return fail( ZPIC_E_INVALID, "null species description" );
+    if ( desc->m_q == 0 ) return fail( ZPIC_E_INVALID, "Invalid m_q value, must be not 0" );          // species.cpp:1698
+    if ( desc->ppc[0] < 1 || desc->ppc[1] < 1 ) return fail( ZPIC_E_INVALID, "Invalid ppc value, must be >= 1 in all directions" );
+    if ( desc->density.type < 0 || desc->density.type > 4 ) return fail( ZPIC_E_INVALID, "invalid density type" );
+    if ( desc->udist.type < 0 || desc->udist.type > 3 ) return fail( ZPIC_E_INVALID, "invalid udist type" );
+    if ( desc->udist.type == ZPIC_UDIST_THERMALCORR && desc->udist.npmin <= 1 )
+        return fail( ZPIC_E_INVALID, "invalid npmin parameter, must be > 1" );                        // udist.h:47-50
+    for ( int a = 0; a < 2; a++ ) {                                                                     // species.h:211-235
+        const int lo = desc->bc[2*a], hi = desc->bc[2*a+1];
+        if ( ( lo == ZPIC_SPECIES_BC_PERIODIC || hi == ZPIC_SPECIES_BC_PERIODIC ) && lo != hi )
+            return fail( ZPIC_E_INVALID, "Species boundary type mismatch" );
+    }
+    if ( s->species.size() >= 32 ) return fail( ZPIC_E_INVALID, "too many species" );
+    s->plan.release();
+    auto sp = std::make_unique<HSpecies>();
+    sp->name = desc->name ? desc->name : "species";
+    sp->m_q = desc->m_q;
+    sp->ppc[0] = desc->ppc[0]; sp->ppc[1] = desc->ppc[1];
+    sp->dens = desc->density;
+    sp->ud = desc->udist;
+    sp->push_type = desc->push_type ? 1 : 0;
+    for ( int k = 0; k < 4; k++ ) sp->bc[k] = desc->bc[k];
+    // Species::initialize (species.cpp:1730-1788)
+    sp->box[0] = s->box[0]; sp->box[1] = s->box[1];
+    sp->dt = (float) s->dt;
+    sp->id = (int) s->species.size() + 1;                          // simulation.h:68-71
+    const float n0 = sp->dens.type == ZPIC_DENSITY_NONE ? 0.f : std::fabs( sp->dens.n0 );
+    sp->q = std::copysign( n0, sp->m_q ) / ( sp->ppc[0] * sp->ppc[1] );
+    const float dimsx = (float) ( s->nxx * s->ntx ), dimsy = (float) ( s->nxy * s->nty );
+    sp->dx[0] = sp->box[0] / dimsx; sp->dx[1] = sp->box[1] / dimsy;
+    const uint64_t ref_max = (uint64_t) ( 1.2 * dimsx * dimsy * sp->ppc[0] * sp->ppc[1] );
+    const int nt = s->ntx * s->nty;
+    // initial particles on the host, reference algorithms and order
+    zbhost::Injector I = injector( s, sp.get() );
+    const unsigned range[4] = { 0, (unsigned) ( s->nxx * s->ntx - 1 ), 0, (unsigned) ( s->nxy * s->nty - 1 ) };
+    std::vector<int> np_inj( nt, 0 ), offset( nt, 0 ), np( nt, 0 );
+    I.count( range, np_inj.data() );
+    long long total = 0;
+    for ( int t = 0; t < nt; t++ ) { offset[t] = (int) total; total += np_inj[t]; }
+    std::vector<int32_t> ix( 2 * total ); std::vector<float> x( 2 * total ), u( 3 * total );
+    I.inject( range, offset.data(), np.data(), ix.data(), x.data(), u.data() );
+    zbhost::udist_set( sp->ud, sp->id, geom( s ), offset.data(), np.data(), ix.data(), u.data() );
+    // capacity: the reference's max_part, raised if the slot layout needs more
+    const int min_slack = std::max<int>( 16, (int) ( sp->ppc[0] * sp->ppc[1] * s->nxx * s->nxy / 8 ) );
+    uint64_t need = 0; for ( int t = 0; t < nt; t++ ) need += roundup4( np[t] );
+    const uint64_t max_part = std::max<uint64_t>( { ref_max, need + (uint64_t) nt * 4, 1024 } );
+    (void) min_slack;
+    TRY( species_alloc( s, sp.get(), max_part ) );
+    species_params( s, sp.get() );
+    sp->d.nchunk = 1;
+    TRY( dalloc( &sp->d.energy, (size_t) nt * 64 ) );
+    CK( cudaMemset( sp->d.energy, 0, (size_t) nt * 64 * sizeof( double ) ) );
+    HSpecies * raw = sp.get();
+    s->species.push_back( sp.release() );
+    // chunking depends on the total tile count of all species
+    int ntot = 0; for ( auto * h : s->species ) ntot += h->ntiles;
+    const int ch = auto_chunks( ntot, s->chunks_opt );
+    for ( auto * h : s->species ) h->d.nchunk = ch;
+    TRY( species_upload( s, raw, np, ix.data(), x.data(), u.data() ) );
+    if ( species_id ) *species_id = (int) s->species.size() - 1;
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_set_moving_window( zpic_sim * s ) {
+    TRY( sim_select( s ) );
+    // Simulation::set_moving_window (simulation.h:56-62): each object checks iter == 0
+    if ( s->emf_iter == 0 ) {
+        s->emf_mw.init( s->dx[0] );
+        s->emf_bc[0] = s->emf_bc[1] = ZPIC_EMF_BC_NONE;
+    }
+    if ( s->cur_iter == 0 ) {
+        s->cur_mw.init( s->dx[0] );
+        s->cur_bc[0] = s->cur_bc[1] = ZPIC_CURRENT_BC_NONE;
+    }
+    for ( auto * sp : s->species ) {
+        if ( sp->iter == 0 ) {
+            sp->mw.init( sp->dx[0] );
+            sp->bc[0] = sp->bc[1] = ZPIC_SPECIES_BC_OPEN;
+            species_params( s, sp );
+        }
+    }
+    TRY( upload_run( s ) );
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_set_option( zpic_sim * s, const char * key, double v ) {
+    TRY( sim_select( s ) );
+    if ( !key ) return fail( ZPIC_E_INVALID, "null option" );
+    std::string k( key );
+    if ( k == "graph" ) { s->use_graph = v != 0; }
+    else if ( k == "profile" ) { s->profile = v != 0; if ( s->profile ) s->use_graph = false; }
+    else if ( k == "chunks" ) {
+        s->chunks_opt = (int) v;
+        int ntot = 0; for ( auto * h : s->species ) ntot += h->ntiles;
+        const int ch = auto_chunks( std::max( 1, ntot ), s->chunks_opt );
+        for ( auto * h : s->species ) {
+            if ( h->d.nchunk != ch ) {
+                dfree( h->d.energy );
+                TRY( dalloc( &h->d.energy, (size_t) h->ntiles * ch ) );
+                CK( cudaMemset( h->d.energy, 0, (size_t) h->ntiles * ch * sizeof( double ) ) );
+                h->d.nchunk = ch;
+            }
+        }
+        s->plan.release();
+    }
+    else return fail( ZPIC_E_INVALID, "unknown option " + k );
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_advance( zpic_sim * s, int32_t nsteps ) {
+    TRY( sim_select( s ) );
+    if ( nsteps < 0 ) return fail( ZPIC_E_INVALID, "negative step count" );
+    TRY( ensure_plan( s ) );
+    // pending fine-grained work must not be mixed with a full step
+    for ( auto * sp : s->species ) {
+        if ( sp->counters_dirty ) {
+            CK( cudaMemsetAsync( sp->d.npt, 0, 9 * sp->ntiles * sizeof( int ), s->stream ) );
+            CK( cudaMemsetAsync( sp->d.nidx, 0, sp->ntiles * sizeof( int ), s->stream ) );
+            sp->counters_dirty = false;
+        }
+    }
+    uint64_t l = 0;
+    TRY( plan_advance( s->plan, s->stream, nsteps, s->use_graph && !s->profile, &l ) );
+    s->launches += l;
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_advance_mov_window( zpic_sim * s, int32_t nsteps ) {
+    TRY( sim_select( s ) );
+    TRY( ensure_plan( s ) );
+    for ( int n = 0; n < nsteps; n++ ) {
+        TRY( ensure_jdep_clean( s, s->stream ) );
+        s->j_final = false;
+        for ( size_t k = 0; k < s->species.size(); k++ ) TRY( species_advance_mw( s, (int) k ) );
+        TRY( run_current( s->plan, s->stream ) );
+        s->cur_iter++;
+        if ( s->cur_mw.needs_move( s->cur_iter * s->dt ) ) s->cur_mw.advance();
+        TRY( run_fields( s->plan, s->stream, 1, 0, 1 ) );
+        s->jdep_clean = true;
+        s->j_final = true;
+        s->emf_iter++;
+        if ( s->emf_mw.active && s->emf_mw.needs_move( s->emf_iter * s->dt ) ) {
+            TRY( run_shift( s->plan, s->stream, 0 ) );
+            s->emf_mw.advance();
+        }
+        s->iter++;
+    }
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_iter( zpic_sim * s, uint32_t * iter ) {
+    if ( !s || !iter ) return fail( ZPIC_E_INVALID, "null argument" );
+    *iter = s->iter;
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_synchronize( zpic_sim * s ) {
+    TRY( sim_select( s ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    return check_status( s );
+}
+
+int zpic_b200_sim_phase_times( zpic_sim * s, double * ms, uint64_t * launches, int32_t n ) {
+    TRY( sim_select( s ) );
+    resolve_phase_events( s );
+    for ( int p = 0; p < n && p < PH_N; p++ ) {
+        if ( ms ) ms[p] = s->phase_ms[p];
+        if ( launches ) launches[p] = s->phase_launches[p];
+    }
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_reset_phase_times( zpic_sim * s ) {
+    TRY( sim_select( s ) );
+    resolve_phase_events( s );
+    for ( int p = 0; p < PH_N; p++ ) { s->phase_ms[p] = 0; s->phase_launches[p] = 0; }
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_launch_count( zpic_sim * s, uint64_t * count ) {
+    if ( !s || !count ) return fail( ZPIC_E_INVALID, "null argument" );
+    *count = s->launches;
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_stream( zpic_sim * s, void ** stream ) {
+    if ( !s || !stream ) return fail( ZPIC_E_INVALID, "null argument" );
+    *stream = (void *) s->stream;
+    return ZPIC_OK;
+}
+
+// ---- EMF ----
+int zpic_b200_emf_set_bc( zpic_sim * s, const int32_t bc[4] ) {
+    TRY( sim_select( s ) );
+    for ( int a = 0; a < 2; a++ )                                   // emf.h:113-130
+        if ( ( bc[2*a] == ZPIC_EMF_BC_PERIODIC || bc[2*a+1] == ZPIC_EMF_BC_PERIODIC ) && bc[2*a] != bc[2*a+1] )
+            return fail( ZPIC_E_INVALID, "EMF boundary type mismatch" );
+    for ( int k = 0; k < 4; k++ ) s->emf_bc[k] = bc[k];
+    return upload_run( s );
+}
+
+int zpic_b200_emf_advance( zpic_sim * s, int32_t with_current ) {
+    TRY( sim_select( s ) );
+    TRY( ensure_plan( s ) );
+    TRY( run_fields( s->plan, s->stream, with_current ? 1 : 0, s->j_final ? 0 : 1, 0 ) );
+    s->emf_iter++;
+    if ( s->emf_mw.active && s->emf_mw.needs_move( s->emf_iter * s->dt ) ) {
+        TRY( run_shift( s->plan, s->stream, 0 ) );
+        s->emf_mw.advance();
+    }
+    CK( cudaStreamSynchronize( s->stream ) );
+    return check_status( s );
+}
+
+int zpic_b200_emf_energy( zpic_sim * s, double ene_E[3], double ene_B[3] ) {
+    TRY( sim_select( s ) );
+    TRY( ensure_plan( s ) );
+    const int nt = s->ntx * s->nty;
+    double * part = nullptr;
+    TRY( dalloc( &part, 6 * (size_t) nt ) );
+    CK( launch_field_energy( s->stream, s->plan.runs_d, 0, nt, part ) );
+    s->launches++;
+    std::vector<double> h( 6 * (size_t) nt );
+    CK( cudaMemcpyAsync( h.data(), part, h.size() * sizeof( double ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    dfree( part );
+    double e[6] = { 0, 0, 0, 0, 0, 0 };
+    for ( int t = 0; t < nt; t++ ) for ( int k = 0; k < 6; k++ ) e[k] += h[6 * (size_t) t + k];   // tile order
+    for ( int k = 0; k < 3; k++ ) { ene_E[k] = e[k]; ene_B[k] = e[3 + k]; }
+    return check_status( s );
+}
+
+int zpic_b200_laser_add( zpic_sim * s, const zpic_laser_desc * l ) {
+    TRY( sim_select( s ) );
+    if ( !l ) return fail( ZPIC_E_INVALID, "null laser" );
+    std::vector<float> E, B;
+    if ( zbhost::laser_fields( *l, geom( s ), s->box, E, B ) < 0 )
+        return fail( ZPIC_E_INVALID, "Invalid laser parameters" );
+    float * tmp = nullptr;
+    TRY( dalloc( &tmp, E.size() ) );
+    CK( cudaMemcpyAsync( tmp, E.data(), E.size() * sizeof( float ), cudaMemcpyHostToDevice, s->stream ) );
+    CK( launch_grid_add( s->stream, s->run.E, tmp, E.size() ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    CK( cudaMemcpyAsync( tmp, B.data(), B.size() * sizeof( float ), cudaMemcpyHostToDevice, s->stream ) );
+    CK( launch_grid_add( s->stream, s->run.B, tmp, B.size() ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    s->launches += 2;
+    dfree( tmp );
+    return ZPIC_OK;
+}
+
+// ---- Current ----
+int zpic_b200_current_set_bc( zpic_sim * s, const int32_t bc[4] ) {
+    TRY( sim_select( s ) );
+    for ( int a = 0; a < 2; a++ )                                   // current.h:95-112
+        if ( ( bc[2*a] == ZPIC_CURRENT_BC_PERIODIC || bc[2*a+1] == ZPIC_CURRENT_BC_PERIODIC ) && bc[2*a] != bc[2*a+1] )
+            return fail( ZPIC_E_INVALID, "Current boundary type mismatch" );
+    for ( int k = 0; k < 4; k++ ) s->cur_bc[k] = bc[k];
+    return upload_run( s );
+}
+
+int zpic_b200_current_set_filter( zpic_sim * s, int32_t type, int32_t dir, uint32_t order ) {
+    TRY( sim_select( s ) );
+    if ( type < 0 || type > 2 ) return fail( ZPIC_E_INVALID, "invalid filter type" );
+    s->ftype = type; s->fdir = dir ? 1 : 0; s->forder = order > 0 ? order : 1;   // filter.h:35
+    s->plan.built = false;
+    return ZPIC_OK;
+}
+
+int zpic_b200_current_zero( zpic_sim * s ) {
+    TRY( sim_select( s ) );
+    s->jdep_clean = false;
+    TRY( ensure_jdep_clean( s, s->stream ) );
+    CK( cudaMemsetAsync( s->run.J, 0, s->grid_floats() * sizeof( float ), s->stream ) );
+    s->j_final = false;
+    return ZPIC_OK;
+}
+
+int zpic_b200_current_advance( zpic_sim * s ) {
+    TRY( sim_select( s ) );
+    TRY( ensure_plan( s ) );
+    TRY( run_current( s->plan, s->stream ) );
+    s->j_final = true;
+    s->cur_iter++;
+    if ( s->cur_mw.needs_move( s->cur_iter * s->dt ) ) s->cur_mw.advance();
+    CK( cudaStreamSynchronize( s->stream ) );
+    return check_status( s );
+}
+
+// ---- Species ----
+int zpic_b200_species_advance( zpic_sim * s, int32_t sp, int32_t mode ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    if ( mode == ZPIC_ADVANCE_FULL ) TRY( species_kernel( s, sp, 1, 2, nullptr ) );
+    else if ( mode == ZPIC_ADVANCE_CURRENT ) TRY( species_kernel( s, sp, 0, 2, nullptr ) );
+    else if ( mode == ZPIC_ADVANCE_FREE ) TRY( species_kernel( s, sp, 0, 1, nullptr ) );
+    else return fail( ZPIC_E_INVALID, "invalid advance mode" );
+    TRY( species_sort( s, sp, 0 ) );
+    s->species[sp]->iter++;
+    s->j_final = false;
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_advance_mov_window( zpic_sim * s, int32_t sp ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    s->j_final = false;
+    return species_advance_mw( s, sp );
+}
+
+int zpic_b200_species_push( zpic_sim * s, int32_t sp ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    return species_kernel( s, sp, 1, 0, nullptr );
+}
+
+int zpic_b200_species_move( zpic_sim * s, int32_t sp ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    s->j_final = false;
+    return species_kernel( s, sp, 0, 2, nullptr );
+}
+
+int zpic_b200_species_process_bc( zpic_sim * s, int32_t sp ) {
+    // Reflecting walls are applied inside the move kernel (after each move),
+    // which is where Species::advance calls process_bc (species.cpp:2060).
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_tile_sort( zpic_sim * s, int32_t sp ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    return species_sort( s, sp, 0 );
+}
+
+int zpic_b200_species_set_bc( zpic_sim * s, int32_t sp, const int32_t bc[4] ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    for ( int a = 0; a < 2; a++ )
+        if ( ( bc[2*a] == ZPIC_SPECIES_BC_PERIODIC || bc[2*a+1] == ZPIC_SPECIES_BC_PERIODIC ) && bc[2*a] != bc[2*a+1] )
+            return fail( ZPIC_E_INVALID, "Species boundary type mismatch" );
+    HSpecies * h = s->species[sp];
+    for ( int k = 0; k < 4; k++ ) h->bc[k] = bc[k];
+    species_params( s, h );
+    s->plan.release();
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_set_push_type( zpic_sim * s, int32_t sp, int32_t type ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    s->species[sp]->push_type = type ? 1 : 0;
+    s->plan.release();
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_energy( zpic_sim * s, int32_t sp, double * energy ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) ); TRY( ensure_plan( s ) );
+    HSpecies * h = s->species[sp];
+    CK( launch_energy_sum( s->stream, s->plan.sps_d, sp, h->ntiles * h->d.nchunk, s->dscratch ) );
+    s->launches++;
+    double d = 0;
+    CK( cudaMemcpyAsync( &d, s->dscratch, sizeof( double ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    *energy = d * h->q * h->m_q * h->dx[0] * h->dx[1];          // species.h:365-368
+    return check_status( s );
+}
+
+int zpic_b200_species_nmove( zpic_sim * s, int32_t sp, uint64_t * nmove ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    unsigned long long v = 0;
+    CK( cudaMemcpyAsync( &v, s->species[sp]->d.nmove, sizeof( v ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    *nmove = v;
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_nmove( zpic_sim * s, uint64_t * nmove ) {
+    TRY( sim_select( s ) );
+    uint64_t t = 0;
+    for ( size_t k = 0; k < s->species.size(); k++ ) { uint64_t v; TRY( zpic_b200_species_nmove( s, (int) k, &v ) ); t += v; }
+    *nmove = t;
+    return ZPIC_OK;
+}
+
+static int np_stats( zpic_sim * s, int sp, unsigned long long out[2] ) {
+    TRY( ensure_plan( s ) );
+    CK( launch_np_stats( s->stream, s->plan.sps_d, sp, (unsigned long long *) s->dscratch ) );
+    s->launches++;
+    CK( cudaMemcpyAsync( out, s->dscratch, 2 * sizeof( unsigned long long ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_np_total( zpic_sim * s, int32_t sp, uint64_t * np ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    unsigned long long st[2]; TRY( np_stats( s, sp, st ) );
+    *np = st[0];
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_np_max_tile( zpic_sim * s, int32_t sp, uint32_t * np ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    unsigned long long st[2]; TRY( np_stats( s, sp, st ) );
+    *np = (uint32_t) st[1];
+    return ZPIC_OK;
+}
+
+static int tiles_host( zpic_sim * s, int sp, std::vector<int> & np, std::vector<int> & poff ) {
+    HSpecies * h = s->species[sp];
+    np.resize( h->ntiles ); poff.resize( h->ntiles );
+    CK( cudaMemcpyAsync( np.data(), h->d.np, h->ntiles * sizeof( int ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    long long o = 0;
+    for ( int t = 0; t < h->ntiles; t++ ) { poff[t] = (int) o; o += np[t]; }
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_get_tiles( zpic_sim * s, int32_t sp, int32_t * np, int32_t * offset ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    std::vector<int> n, o;
+    TRY( tiles_host( s, sp, n, o ) );
+    if ( np ) std::memcpy( np, n.data(), n.size() * sizeof( int ) );
+    if ( offset ) std::memcpy( offset, o.data(), o.size() * sizeof( int ) );
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_get( zpic_sim * s, int32_t sp, int32_t * ix, float * x, float * u ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) ); TRY( ensure_plan( s ) );
+    HSpecies * h = s->species[sp];
+    std::vector<int> n, o;
+    TRY( tiles_host( s, sp, n, o ) );
+    const size_t total = (size_t) o.back() + n.back();
+    int * poff_d = nullptr; int2 * ix_d = nullptr; float2 * x_d = nullptr; float * u_d = nullptr;
+    TRY( dalloc( &poff_d, h->ntiles ) ); TRY( dalloc( &ix_d, total ) ); TRY( dalloc( &x_d, total ) ); TRY( dalloc( &u_d, 3 * total ) );
+    CK( cudaMemcpyAsync( poff_d, o.data(), o.size() * sizeof( int ), cudaMemcpyHostToDevice, s->stream ) );
+    CK( launch_pack( s->stream, sp, h->ntiles, s->plan.sps_d, poff_d, ix_d, x_d, u_d ) );
+    s->launches++;
+    if ( total ) {
+        CK( cudaMemcpyAsync( ix, ix_d, total * sizeof( int2 ), cudaMemcpyDeviceToHost, s->stream ) );
+        CK( cudaMemcpyAsync( x, x_d, total * sizeof( float2 ), cudaMemcpyDeviceToHost, s->stream ) );
+        CK( cudaMemcpyAsync( u, u_d, 3 * total * sizeof( float ), cudaMemcpyDeviceToHost, s->stream ) );
+    }
+    CK( cudaStreamSynchronize( s->stream ) );
+    dfree( poff_d ); dfree( ix_d ); dfree( x_d ); dfree( u_d );
+    return check_status( s );
+}
+
+int zpic_b200_species_set( zpic_sim * s, int32_t sp, const int32_t * np, const int32_t * ix, const float * x, const float * u ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    HSpecies * h = s->species[sp];
+    std::vector<int> n( np, np + h->ntiles );
+    for ( int v : n ) if ( v < 0 ) return fail( ZPIC_E_INVALID, "negative particle count" );
+    CK( cudaStreamSynchronize( s->stream ) );
+    TRY( species_upload( s, h, n, ix, x, u ) );
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_gather( zpic_sim * s, int32_t sp, int32_t quant, float * out ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) ); TRY( ensure_plan( s ) );
+    if ( quant < 0 || quant > 4 ) return fail( ZPIC_E_INVALID, "invalid quantity" );
+    HSpecies * h = s->species[sp];
+    std::vector<int> n, o;
+    TRY( tiles_host( s, sp, n, o ) );
+    const size_t total = (size_t) o.back() + n.back();
+    int * poff_d = nullptr; float * out_d = nullptr;
+    TRY( dalloc( &poff_d, h->ntiles ) ); TRY( dalloc( &out_d, total ) );
+    CK( cudaMemcpyAsync( poff_d, o.data(), o.size() * sizeof( int ), cudaMemcpyHostToDevice, s->stream ) );
+    // Species::gather scales positions by dx (species.h:510-526)
+    const int scaled = quant <= 1;
+    const float sx = quant == 0 ? h->dx[0] : h->dx[1];
+    CK( launch_gather( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, poff_d, quant, sx, 0.f, scaled, out_d ) );
+    s->launches++;
+    if ( total ) CK( cudaMemcpyAsync( out, out_d, total * sizeof( float ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    dfree( poff_d ); dfree( out_d );
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_charge( zpic_sim * s, int32_t sp, float * out ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) ); TRY( ensure_plan( s ) );
+    HSpecies * h = s->species[sp];
+    const int cextx = s->nxx + 1, cexty = s->nxy + 1;
+    const int cvol = roundup4( cextx * cexty );
+    const size_t nraw = (size_t) cvol * h->ntiles;
+    const size_t ndense = (size_t) s->ntx * s->nxx * s->nty * s->nxy;
+    float * raw = nullptr; float * dense = nullptr;
+    TRY( dalloc( &raw, nraw ) ); TRY( dalloc( &dense, ndense ) );
+    CK( cudaMemsetAsync( raw, 0, nraw * sizeof( float ), s->stream ) );
+    CK( launch_dep_charge( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, raw, cextx, cvol ) );
+    // the charge grid is a new grid object, hence periodic (grid.h:79)
+    CK( launch_charge_finish( s->stream, raw, dense, s->ntx, s->nty, s->nxx, s->nxy, cextx, cvol, 1, 1 ) );
+    s->launches += 2;
+    CK( cudaMemcpyAsync( out, dense, ndense * sizeof( float ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    dfree( raw ); dfree( dense );
+    return ZPIC_OK;
+}
+
+// ---- grids ----
+static float * grid_ptr( zpic_sim * s, int which, bool for_read ) {
+    switch ( which ) {
+    case ZPIC_GRID_E: return s->run.E;
+    case ZPIC_GRID_B: return s->run.B;
+    case ZPIC_GRID_J: return ( for_read && !s->j_final ) ? s->run.Jdep : s->run.J;
+    }
+    return nullptr;
+}
+
+int zpic_b200_grid_size( zpic_sim * s, int32_t which, uint64_t * cells ) {
+    if ( !s || !cells || which < 0 || which > 2 ) return fail( ZPIC_E_INVALID, "invalid argument" );
+    *cells = (uint64_t) s->run.tile_vol * s->ntx * s->nty;
+    return ZPIC_OK;
+}
+
+int zpic_b200_grid_get( zpic_sim * s, int32_t which, float * out ) {
+    TRY( sim_select( s ) );
+    float * p = grid_ptr( s, which, true );
+    if ( !p || !out ) return fail( ZPIC_E_INVALID, "invalid grid" );
+    CK( cudaMemcpyAsync( out, p, s->grid_floats() * sizeof( float ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    return ZPIC_OK;
+}
+
+int zpic_b200_grid_set( zpic_sim * s, int32_t which, const float * in ) {
+    TRY( sim_select( s ) );
+    // J: the buffer grid_get returns (raw deposits before Current::advance, else the summed current)
+    float * p = grid_ptr( s, which, true );
+    if ( !p || !in ) return fail( ZPIC_E_INVALID, "invalid grid" );
+    CK( cudaMemcpyAsync( p, in, s->grid_floats() * sizeof( float ), cudaMemcpyHostToDevice, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    if ( which == ZPIC_GRID_J && !s->j_final ) s->jdep_clean = false;
+    return ZPIC_OK;
+}
+
+int zpic_b200_grid_gather( zpic_sim * s, int32_t which, int32_t fc, float * out ) {
+    TRY( sim_select( s ) );
+    float * p = grid_ptr( s, which, true );
+    if ( !p || !out || fc < 0 || fc > 2 ) return fail( ZPIC_E_INVALID, "invalid grid" );
+    const size_t n = (size_t) s->ntx * s->nxx * s->nty * s->nxy;
+    float * d = nullptr;
+    TRY( dalloc( &d, n ) );
+    CK( launch_grid_gather( s->stream, p, d, fc, s->ntx, s->nty, s->nxx, s->nxy, s->run.extx, s->run.gc_off, s->run.tile_vol ) );
+    s->launches++;
+    CK( cudaMemcpyAsync( out, d, n * sizeof( float ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    dfree( d );
+    return ZPIC_OK;
+}
+
+// ---- batches ----
+int zpic_b200_batch_create( zpic_sim * const * sims, int32_t n, zpic_batch ** out ) {
+    if ( !sims || n <= 0 || !out ) return fail( ZPIC_E_INVALID, "invalid batch" );
+    auto b = std::make_unique<zpic_batch>();
+    for ( int i = 0; i < n; i++ ) {
+        if ( !sims[i] ) return fail( ZPIC_E_INVALID, "null simulation in batch" );
+        if ( sims[i]->device != sims[0]->device ) return fail( ZPIC_E_INVALID, "batch simulations must share a device" );
+        if ( sims[i]->emf_mw.active ) return fail( ZPIC_E_INVALID, "moving-window simulations cannot be batched" );
+        b->sims.push_back( sims[i] );
+    }
+    CK( cudaSetDevice( sims[0]->device ) );
+    CK( cudaStreamCreateWithFlags( &b->stream, cudaStreamNonBlocking ) );
+    CK( cudaEventCreateWithFlags( &b->ev, cudaEventDisableTiming ) );
+    TRY( plan_build( b->plan, b->sims ) );
+    *out = b.release();
+    return ZPIC_OK;
+}
+
+int zpic_b200_batch_advance( zpic_batch * b, int32_t nsteps ) {
+    if ( !b ) return fail( ZPIC_E_INVALID, "null batch" );
+    CK( cudaSetDevice( b->sims[0]->device ) );
+    for ( auto * s : b->sims ) {
+        if ( !s->plan.built ) TRY( ensure_plan( s ) );
+        CK( cudaEventRecord( b->ev, s->stream ) );
+        CK( cudaStreamWaitEvent( b->stream, b->ev, 0 ) );
+        for ( auto * sp : s->species )
+            if ( sp->counters_dirty ) {
+                CK( cudaMemsetAsync( sp->d.npt, 0, 9 * sp->ntiles * sizeof( int ), b->stream ) );
+                CK( cudaMemsetAsync( sp->d.nidx, 0, sp->ntiles * sizeof( int ), b->stream ) );
+                sp->counters_dirty = false;
+            }
+    }
+    uint64_t l = 0;
+    TRY( plan_advance( b->plan, b->stream, nsteps, true, &l ) );
+    CK( cudaEventRecord( b->ev, b->stream ) );
+    for ( auto * s : b->sims ) {
+        CK( cudaStreamWaitEvent( s->stream, b->ev, 0 ) );
+        s->launches += l / b->sims.size();
+    }
+    return ZPIC_OK;
+}
+
+int zpic_b200_batch_synchronize( zpic_batch * b ) {
+    if ( !b ) return fail( ZPIC_E_INVALID, "null batch" );
+    CK( cudaSetDevice( b->sims[0]->device ) );
+    CK( cudaStreamSynchronize( b->stream ) );
+    for ( auto * s : b->sims ) TRY( check_status( s ) );
+    return ZPIC_OK;
+}
+
+int zpic_b200_batch_destroy( zpic_batch * b ) {
+    if ( !b ) return ZPIC_OK;
+    cudaSetDevice( b->sims[0]->device );
+    cudaStreamSynchronize( b->stream );
+    b->plan.release();
+    cudaEventDestroy( b->ev );
+    cudaStreamDestroy( b->stream );
+    delete b;
+    return ZPIC_OK;
+}
+
+}  // extern "C"

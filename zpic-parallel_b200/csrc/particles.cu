@@ -1,0 +1,999 @@
+// particles.cu -- particle kernels of the em2d step for sm_100a.
+//
+// Compiled with -fmad=false: no implicit FMA contraction.  The reference
+// build (g++ -std=c++17) contracts nothing either and uses explicit fused
+// multiply-adds only through ops::fma (utils.h:105-136), mirrored here with
+// __fmaf_rn; division and square root stay IEEE (no fast-math).  A particle's
+// push and move are therefore bit-identical to the reference.
+#include "zpic_dev.cuh"
+
+namespace zb {
+
+// ---------------------------------------------------------------------------
+// Per-particle physics
+// ---------------------------------------------------------------------------
+
+// 1 / Lorentz gamma (species.cpp:22-26)
+__device__ __forceinline__ float rgamma( float ux, float uy, float uz ) {
+    return 1.0f / sqrtf( __fmaf_rn( uz, uz, __fmaf_rn( uy, uy, __fmaf_rn( ux, ux, 1.0f ) ) ) );
+}
+
+// Linear interpolation of the staggered Yee fields (species.cpp:43-92).
+// E, B point at cell (0,0) of float3 AoS tiles in shared memory.
+__device__ __forceinline__ void interpolate_fld( const float * __restrict__ E, const float * __restrict__ B,
+                                                 int ys, int i, int j, float xx, float xy,
+                                                 float & ex, float & ey, float & ez,
+                                                 float & bx, float & by, float & bz ) {
+    const float s0x = 0.5f - xx, s1x = 0.5f + xx;
+    const float s0y = 0.5f - xy, s1y = 0.5f + xy;
+    const int hx = xx < 0, hy = xy < 0;
+    const int ih = i - hx, jh = j - hy;
+    const float s0xh = ( 1 - hx ) - xx, s1xh = ( hx ) + xx;
+    const float s0yh = ( 1 - hy ) - xy, s1yh = ( hy ) + xy;
+#define F3( A, c, k ) ( A[ 3 * ( c ) + ( k ) ] )
+    ex = ( F3( E, ih +     j*ys, 0 ) * s0xh + F3( E, ih+1 +     j*ys, 0 ) * s1xh ) * s0y +
+         ( F3( E, ih + (j+1)*ys, 0 ) * s0xh + F3( E, ih+1 + (j+1)*ys, 0 ) * s1xh ) * s1y;
+    ey = ( F3( E, i  +    jh*ys, 1 ) * s0x  + F3( E, i+1  +    jh*ys, 1 ) * s1x  ) * s0yh +
+         ( F3( E, i  + (jh+1)*ys, 1 ) * s0x + F3( E, i+1  + (jh+1)*ys, 1 ) * s1x  ) * s1yh;
+    ez = ( F3( E, i  +     j*ys, 2 ) * s0x  + F3( E, i+1  +     j*ys, 2 ) * s1x  ) * s0y +
+         ( F3( E, i  + (j+1)*ys, 2 ) * s0x  + F3( E, i+1  + (j+1)*ys, 2 ) * s1x  ) * s1y;
+    bx = ( F3( B, i  +    jh*ys, 0 ) * s0x  + F3( B, i+1  +    jh*ys, 0 ) * s1x  ) * s0yh +
+         ( F3( B, i  + (jh+1)*ys, 0 ) * s0x + F3( B, i+1  + (jh+1)*ys, 0 ) * s1x  ) * s1yh;
+    by = ( F3( B, ih +     j*ys, 1 ) * s0xh + F3( B, ih+1 +     j*ys, 1 ) * s1xh ) * s0y +
+         ( F3( B, ih + (j+1)*ys, 1 ) * s0xh + F3( B, ih+1 + (j+1)*ys, 1 ) * s1xh ) * s1y;
+    bz = ( F3( B, ih +    jh*ys, 2 ) * s0xh + F3( B, ih+1 +    jh*ys, 2 ) * s1xh ) * s0yh +
+         ( F3( B, ih + (jh+1)*ys, 2 ) * s0xh + F3( B, ih+1 + (jh+1)*ys, 2 ) * s1xh ) * s1yh;
+#undef F3
+}
+
+// Relativistic Boris push with tangent-linearised rotation (species.cpp:117-178)
+__device__ __forceinline__ void dudt_boris( float alpha, float ex, float ey, float ez,
+                                            float bx, float by, float bz,
+                                            float & ux, float & uy, float & uz, double & energy ) {
+    ex *= alpha; ey *= alpha; ez *= alpha;
+    float utx = ux + ex, uty = uy + ey, utz = uz + ez;
+    {
+        const float utsq = __fmaf_rn( utz, utz, __fmaf_rn( uty, uty, utx * utx ) );
+        const float gamma = sqrtf( 1.0f + utsq );
+        energy += (double) ( utsq / ( gamma + 1.0f ) );
+        const float alpha_gamma = alpha / gamma;
+        bx *= alpha_gamma; by *= alpha_gamma; bz *= alpha_gamma;
+    }
+    float vx = __fmaf_rn( bz, uty, utx );
+    float vy = __fmaf_rn( bx, utz, uty );
+    float vz = __fmaf_rn( by, utx, utz );
+    vx = __fmaf_rn( -by, utz, vx );
+    vy = __fmaf_rn( -bz, utx, vy );
+    vz = __fmaf_rn( -bx, uty, vz );
+    {
+        const float otsq = 2.0f / __fmaf_rn( bz, bz, __fmaf_rn( by, by, __fmaf_rn( bx, bx, 1.0f ) ) );
+        bx *= otsq; by *= otsq; bz *= otsq;
+    }
+    utx = __fmaf_rn( bz, vy, utx );
+    uty = __fmaf_rn( bx, vz, uty );
+    utz = __fmaf_rn( by, vx, utz );
+    utx = __fmaf_rn( -by, vz, utx );
+    uty = __fmaf_rn( -bz, vx, uty );
+    utz = __fmaf_rn( -bx, vy, utz );
+    ux = utx + ex; uy = uty + ey; uz = utz + ez;
+}
+
+// Boris push with exact Euler-Rodrigues rotation (species.cpp:193-254)
+__device__ __forceinline__ void dudt_boris_euler( float alpha, float ex, float ey, float ez,
+                                                  float bx, float by, float bz,
+                                                  float & ux, float & uy, float & uz, double & energy ) {
+    ex *= alpha; ey *= alpha; ez *= alpha;
+    const float utx = ux + ex, uty = uy + ey, utz = uz + ez;
+    {
+        const float utsq = __fmaf_rn( utz, utz, __fmaf_rn( uty, uty, utx * utx ) );
+        const float gamma = sqrtf( 1.0f + utsq );
+        energy += (double) ( utsq / ( gamma + 1.0f ) );
+        const float alpha2_gamma = ( alpha * 2 ) / gamma;
+        bx *= alpha2_gamma; by *= alpha2_gamma; bz *= alpha2_gamma;
+    }
+    const float bnorm = sqrtf( __fmaf_rn( bx, bx, __fmaf_rn( by, by, bz * bz ) ) );
+    const float s = -( ( bnorm > 0 ) ? sinf( bnorm / 2 ) / bnorm : 1 );
+    const float ra = cosf( bnorm / 2 );
+    const float rb = bx * s, rc = by * s, rd = bz * s;
+    const float r11 =     __fmaf_rn( ra, ra, rb * rb ) - __fmaf_rn( rc, rc, rd * rd );
+    const float r12 = 2 * __fmaf_rn( rb, rc, ra * rd );
+    const float r13 = 2 * __fmaf_rn( rb, rd, -ra * rc );
+    const float r21 = 2 * __fmaf_rn( rb, rc, -ra * rd );
+    const float r22 =     __fmaf_rn( ra, ra, rc * rc ) - __fmaf_rn( rb, rb, rd * rd );
+    const float r23 = 2 * __fmaf_rn( rc, rd, ra * rb );
+    const float r31 = 2 * __fmaf_rn( rb, rd, ra * rc );
+    const float r32 = 2 * __fmaf_rn( rc, rd, -ra * rb );
+    const float r33 =     __fmaf_rn( ra, ra, rd * rd ) - __fmaf_rn( rb, rb, -rc * rc );
+    ux = __fmaf_rn( r11, utx, __fmaf_rn( r21, uty, r31 * utz ) ) + ex;
+    uy = __fmaf_rn( r12, utx, __fmaf_rn( r22, uty, r32 * utz ) ) + ey;
+    uz = __fmaf_rn( r13, utx, __fmaf_rn( r23, uty, r33 * utz ) ) + ez;
+}
+
+// Charge-conserving current of one segment inside one cell (species.cpp:267-310),
+// accumulated into the shared-memory tile current with shared atomics.
+template < typename JT >
+__device__ __forceinline__ void dep_current_seg( int ix, int iy, float x0x, float x0y, float x1x, float x1y,
+                                                 float qnxx, float qnxy, float qvz, JT * J, int stride ) {
+    const float S0x0 = 0.5f - x0x, S0x1 = 0.5f + x0x;
+    const float S1x0 = 0.5f - x1x, S1x1 = 0.5f + x1x;
+    const float S0y0 = 0.5f - x0y, S0y1 = 0.5f + x0y;
+    const float S1y0 = 0.5f - x1y, S1y1 = 0.5f + x1y;
+    const float wl1 = qnxx * ( x1x - x0x );
+    const float wl2 = qnxy * ( x1y - x0y );
+    const float wp10 = 0.5f * ( S0y0 + S1y0 ), wp11 = 0.5f * ( S0y1 + S1y1 );
+    const float wp20 = 0.5f * ( S0x0 + S1x0 ), wp21 = 0.5f * ( S0x1 + S1x1 );
+    JT * Js = J + 3 * ( ix + stride * iy );
+    const int s3 = 3 * stride;
+    atomicAdd( Js + 0,      (JT) ( wl1 * wp10 ) );
+    atomicAdd( Js + 1,      (JT) ( wl2 * wp20 ) );
+    atomicAdd( Js + 2,      (JT) ( qvz * ( S0x0 * S0y0 + S1x0 * S1y0 + ( S0x0 * S1y0 - S1x0 * S0y0 ) / 2.0f ) ) );
+    atomicAdd( Js + 3 + 1,  (JT) ( wl2 * wp21 ) );
+    atomicAdd( Js + 3 + 2,  (JT) ( qvz * ( S0x1 * S0y0 + S1x1 * S1y0 + ( S0x1 * S1y0 - S1x1 * S0y0 ) / 2.0f ) ) );
+    atomicAdd( Js + s3 + 0, (JT) ( wl1 * wp11 ) );
+    atomicAdd( Js + s3 + 2, (JT) ( qvz * ( S0x0 * S0y1 + S1x0 * S1y1 + ( S0x0 * S1y1 - S1x0 * S0y1 ) / 2.0f ) ) );
+    atomicAdd( Js + s3 + 5, (JT) ( qvz * ( S0x1 * S0y1 + S1x1 * S1y1 + ( S0x1 * S1y1 - S1x1 * S0y1 ) / 2.0f ) ) );
+}
+
+// Move one particle, split its trajectory into <= 3 single-cell segments and
+// deposit them (species.cpp:336-430 split2d, 1400-1493 move_deposit_kernel).
+template < bool DEPOSIT, typename JT >
+__device__ __forceinline__ void move_particle( float ux, float uy, float uz, int & ix, int & iy,
+                                               float & xx, float & xy,
+                                               float dt_dx, float dt_dy, float q, float qnxx, float qnxy,
+                                               JT * J, int stride ) {
+    const float rg = rgamma( ux, uy, uz );
+    const float dx = dt_dx * rg * ux;
+    const float dy = dt_dy * rg * uy;
+    const float x0x = xx, x0y = xy;
+    float x1x = x0x + dx, x1y = x0y + dy;
+    const int dix = ( ( x1x >= 0.5f ) - ( x1x < -0.5f ) );
+    const int diy = ( ( x1y >= 0.5f ) - ( x1y < -0.5f ) );
+    if ( DEPOSIT ) {
+        const float qvz = q * uz * rg * 0.5f;
+        const int crossx = dix != 0, crossy = diy != 0;
+        // segment 0 (always), 1 (any crossing), 2 (both crossings)
+        int v0x = ix, v0y = iy;  float v0x0 = x0x, v0y0 = x0y, v0x1 = x1x, v0y1 = x1y, v0q = qvz;
+        int v1x = 0, v1y = 0;    float v1x0 = 0, v1y0 = 0, v1x1 = 0, v1y1 = 0, v1q = 0;
+        int v2x = 0, v2y = 0;    float v2x0 = 0, v2y0 = 0, v2x1 = 0, v2y1 = 0, v2q = 0;
+        if ( crossy && !crossx ) {
+            const float yint = 0.5f * diy;
+            const float eps = ( yint - x0y ) / dy;
+            const float xint = x0x + dx * eps;
+            v0x1 = xint; v0y1 = yint; v0q = qvz * eps;
+            v1x = ix; v1y = iy + diy;
+            v1x0 = xint; v1y0 = -yint;
+            v1x1 = x1x; v1y1 = x1y - diy;
+            v1q = qvz * ( 1 - eps );
+        }
+        if ( crossx ) {
+            const float xint = 0.5f * dix;
+            float eps = ( xint - x0x ) / dx;
+            const float yint = x0y + dy * eps;
+            v0x1 = xint; v0y1 = yint; v0q = qvz * eps;
+            v1x = ix + dix; v1y = iy;
+            v1x0 = -xint; v1y0 = yint;
+            v1x1 = x1x - dix; v1y1 = x1y;
+            v1q = qvz * ( 1 - eps );
+            if ( crossy ) {
+                const float yint2 = 0.5f * diy;
+                if ( yint >= -0.5f && yint < 0.5f ) {
+                    eps = ( yint2 - yint ) / ( x1y - yint );
+                    const float xint2 = -xint + ( x1x - xint ) * eps;
+                    v2x = v1x; v2y = v1y + diy;
+                    v2x0 = xint2; v2y0 = -yint2;
+                    v2x1 = v1x1; v2y1 = v1y1 - diy;
+                    v2q = v1q * ( 1 - eps );
+                    v1x1 = xint2; v1y1 = yint2;
+                    v1q *= eps;
+                } else {
+                    eps = ( yint2 - x0y ) / ( yint - x0y );
+                    const float xint2 = x0x + ( xint - x0x ) * eps;
+                    v2x = v0x; v2y = v0y + diy;
+                    v2x0 = xint2; v2y0 = -yint2;
+                    v2x1 = v0x1; v2y1 = v0y1 - diy;
+                    v2q = v0q * ( 1 - eps );
+                    v0x1 = xint2; v0y1 = yint2;
+                    v0q *= eps;
+                    v1y += diy;
+                    v1y0 -= diy;
+                    v1y1 -= diy;
+                }
+            }
+        }
+        dep_current_seg( v0x, v0y, v0x0, v0y0, v0x1, v0y1, qnxx, qnxy, v0q, J, stride );
+        if ( crossx || crossy ) dep_current_seg( v1x, v1y, v1x0, v1y0, v1x1, v1y1, qnxx, qnxy, v1q, J, stride );
+        if ( crossx && crossy ) dep_current_seg( v2x, v2y, v2x0, v2y0, v2x1, v2y1, qnxx, qnxy, v2q, J, stride );
+    }
+    x1x -= dix; x1y -= diy;
+    xx = x1x; xy = x1y;
+    ix += dix; iy += diy;
+}
+
+// ---------------------------------------------------------------------------
+// Fused particle kernel: push -> move/deposit -> reflecting walls -> leaver
+// detection, one CTA per (species, tile, chunk) work item.
+//
+//   PUSH   0 none, 1 Boris, 2 Boris with Euler-Rodrigues rotation
+//   MOVE   0 none, 1 move (free streaming), 2 move + deposit
+//   DETECT record leavers (bnd_check, particles.cpp:212-303)
+//
+// E and B tiles (guard cells included, the contiguous tile_vol block) are
+// staged into shared memory with one bulk asynchronous copy each; the tile
+// current is accumulated in shared memory and added to the raw current
+// buffer with one bulk reduce-add.  Each thread handles 4 consecutive
+// particles with 128-bit loads and stores.
+// ---------------------------------------------------------------------------
+constexpr int PK_THREADS = 256;
+
+template < int PUSH, int MOVE, bool DETECT >
+__global__ void __launch_bounds__( PK_THREADS )
+k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
+             const RunDev * __restrict__ runs, const int * __restrict__ shifts )
+{
+    extern __shared__ __align__( 16 ) unsigned char smem_raw[];
+    const Item it = items[ blockIdx.x ];
+    const SpDev & S = sps[ it.sp ];
+    const RunDev & R = runs[ S.run ];
+    const int tv = R.tile_vol;
+    const int t = it.tile;
+    const int nchunk = S.nchunk;
+
+    float * sE = reinterpret_cast<float *>( smem_raw );
+    float * sB = sE + 3 * tv;
+    float * sJ = sB + 3 * tv;
+    uint64_t * bar = reinterpret_cast<uint64_t *>( sJ + 3 * tv );
+    double * sred = reinterpret_cast<double *>( bar + 1 );
+
+    const int np = S.np[ t ];
+    const int off = S.off[ t ];
+    const int per = ( ( np + nchunk - 1 ) / nchunk + 3 ) & ~3;
+    const int begin = it.chunk * per;
+    const int end = min( np, begin + per );
+    const int eidx = t * nchunk + it.chunk;
+
+    if ( begin >= end ) {
+        if ( PUSH && threadIdx.x == 0 ) S.energy[ eidx ] = 0.0;
+        return;
+    }
+
+    if ( PUSH ) {
+        if ( threadIdx.x == 0 ) {
+            mbar_init( bar, 1 );
+            fence_mbar_init();
+        }
+        __syncthreads();
+        if ( threadIdx.x == 0 ) {
+            const uint32_t bytes = 12u * tv;
+            mbar_arrive_expect_tx( bar, 2 * bytes );
+            bulk_g2s( sE, R.E + (size_t) t * 3 * tv, bytes, bar );
+            bulk_g2s( sB, R.B + (size_t) t * 3 * tv, bytes, bar );
+        }
+    }
+    if ( MOVE == 2 ) {
+        for ( int i = threadIdx.x; i < 3 * tv; i += blockDim.x ) sJ[i] = 0.0f;
+    }
+    if ( PUSH ) mbar_wait_bounded( bar, 0, R.status );
+    __syncthreads();
+
+    const int ys = R.extx;
+    const float * Ec = sE + 3 * R.gc_off;
+    const float * Bc = sB + 3 * R.gc_off;
+    float * Jc = sJ + 3 * R.gc_off;
+    const int nxx = R.nxx, nxy = R.nxy;
+    const int tx = t % R.ntx, ty = t / R.ntx;
+    const int shift = ( MOVE && shifts ) ? shifts[ it.sp ] : 0;
+    const bool euler = ( PUSH == 2 );
+
+    // reflecting walls handled here (species.cpp:1854-1989): lower rule on the
+    // first tile column, upper rule on the last one; x first, then y.
+    const int rxl = ( MOVE && tx == 0 && ( S.bc[0] > 1 || S.bc[1] > 1 ) && S.bc[0] == 2 );
+    const int rxu = ( MOVE && tx != 0 && tx == R.ntx - 1 && ( S.bc[0] > 1 || S.bc[1] > 1 ) && S.bc[1] == 2 );
+    const int ryl = ( MOVE && ty == 0 && ( S.bc[2] > 1 || S.bc[3] > 1 ) && S.bc[2] == 2 );
+    const int ryu = ( MOVE && ty != 0 && ty == R.nty - 1 && ( S.bc[2] > 1 || S.bc[3] > 1 ) && S.bc[3] == 2 );
+
+    const float alpha = S.alpha;
+    const float dt_dx = S.dt_dx, dt_dy = S.dt_dy, q = S.q, qnxx = S.qnx, qnxy = S.qny;
+
+    uint32_t * __restrict__ pc = S.A.cell + off;
+    float * __restrict__ pxx = S.A.xx + off;
+    float * __restrict__ pxy = S.A.xy + off;
+    float * __restrict__ pux = S.A.ux + off;
+    float * __restrict__ puy = S.A.uy + off;
+    float * __restrict__ puz = S.A.uz + off;
+
+    double energy = 0.0;
+    const int lane = threadIdx.x & 31;
+
+    for ( int b0 = begin; b0 < end; b0 += 4 * blockDim.x ) {
+        const int base = b0 + 4 * threadIdx.x;
+        const int n = max( 0, min( 4, end - base ) );
+        uint32_t c[4]; float x0[4], x1[4], u0[4], u1[4], u2[4];
+        if ( n == 4 ) {
+            uint4 vc = *reinterpret_cast<const uint4 *>( pc + base );
+            c[0] = vc.x; c[1] = vc.y; c[2] = vc.z; c[3] = vc.w;
+            float4 v;
+            v = *reinterpret_cast<const float4 *>( pxx + base ); x0[0] = v.x; x0[1] = v.y; x0[2] = v.z; x0[3] = v.w;
+            v = *reinterpret_cast<const float4 *>( pxy + base ); x1[0] = v.x; x1[1] = v.y; x1[2] = v.z; x1[3] = v.w;
+            if ( PUSH || MOVE ) {
+                v = *reinterpret_cast<const float4 *>( pux + base ); u0[0] = v.x; u0[1] = v.y; u0[2] = v.z; u0[3] = v.w;
+                v = *reinterpret_cast<const float4 *>( puy + base ); u1[0] = v.x; u1[1] = v.y; u1[2] = v.z; u1[3] = v.w;
+                v = *reinterpret_cast<const float4 *>( puz + base ); u2[0] = v.x; u2[1] = v.y; u2[2] = v.z; u2[3] = v.w;
+            }
+        } else {
+#pragma unroll
+            for ( int k = 0; k < 4; k++ ) {
+                if ( k < n ) {
+                    c[k] = pc[ base + k ]; x0[k] = pxx[ base + k ]; x1[k] = pxy[ base + k ];
+                    if ( PUSH || MOVE ) { u0[k] = pux[ base + k ]; u1[k] = puy[ base + k ]; u2[k] = puz[ base + k ]; }
+                } else {
+                    c[k] = 0; x0[k] = x1[k] = 0.f; u0[k] = u1[k] = u2[k] = 0.f;
+                }
+            }
+        }
+
+        int leave_dir[4];
+#pragma unroll
+        for ( int k = 0; k < 4; k++ ) {
+            leave_dir[k] = 4;
+            if ( ( PUSH || MOVE ) && k < n ) {
+                // Sorted particles sit inside their tile; anything else (only
+                // reachable by moving twice without a sort) is flagged and left
+                // untouched so no field or current access leaves the tile block.
+                const int cx0 = cell_x( c[k] ), cy0 = cell_y( c[k] );
+                if ( cx0 < 0 || cx0 >= nxx || cy0 < 0 || cy0 >= nxy ) {
+                    atomicOr( R.status, ST_BAD_CELL );
+                    continue;
+                }
+            }
+            if ( k < n ) {
+                int ix = cell_x( c[k] ), iy = cell_y( c[k] );
+                if ( PUSH ) {
+                    float ex, ey, ez, bx, by, bz;
+                    interpolate_fld( Ec, Bc, ys, ix, iy, x0[k], x1[k], ex, ey, ez, bx, by, bz );
+                    if ( euler ) dudt_boris_euler( alpha, ex, ey, ez, bx, by, bz, u0[k], u1[k], u2[k], energy );
+                    else         dudt_boris( alpha, ex, ey, ez, bx, by, bz, u0[k], u1[k], u2[k], energy );
+                }
+                if ( MOVE ) {
+                    move_particle< MOVE == 2 >( u0[k], u1[k], u2[k], ix, iy, x0[k], x1[k],
+                                                dt_dx, dt_dy, q, qnxx, qnxy, Jc, ys );
+                    ix += shift;
+                    if ( rxl && ix < 0 )    { ix += 1; x0[k] = -x0[k]; u0[k] = -u0[k]; }
+                    if ( rxu && ix >= nxx ) { ix -= 1; x0[k] = -x0[k]; u0[k] = -u0[k]; }
+                    if ( ryl && iy < 0 )    { iy += 1; x1[k] = -x1[k]; u1[k] = -u1[k]; }
+                    if ( ryu && iy >= nxy ) { iy -= 1; x1[k] = -x1[k]; u1[k] = -u1[k]; }
+                    c[k] = pack_cell( ix, iy );
+                }
+                if ( DETECT ) {
+                    const int xcross = ( ix >= nxx ) - ( ix < 0 );
+                    const int ycross = ( iy >= nxy ) - ( iy < 0 );
+                    leave_dir[k] = ( ycross + 1 ) * 3 + ( xcross + 1 );
+                }
+            }
+        }
+
+        if ( MOVE || PUSH ) {
+            if ( n == 4 ) {
+                if ( MOVE ) {
+                    *reinterpret_cast<uint4 *>( pc + base ) = make_uint4( c[0], c[1], c[2], c[3] );
+                    *reinterpret_cast<float4 *>( pxx + base ) = make_float4( x0[0], x0[1], x0[2], x0[3] );
+                    *reinterpret_cast<float4 *>( pxy + base ) = make_float4( x1[0], x1[1], x1[2], x1[3] );
+                }
+                if ( PUSH || rxl || rxu ) *reinterpret_cast<float4 *>( pux + base ) = make_float4( u0[0], u0[1], u0[2], u0[3] );
+                if ( PUSH || ryl || ryu ) *reinterpret_cast<float4 *>( puy + base ) = make_float4( u1[0], u1[1], u1[2], u1[3] );
+                if ( PUSH ) *reinterpret_cast<float4 *>( puz + base ) = make_float4( u2[0], u2[1], u2[2], u2[3] );
+            } else {
+#pragma unroll
+                for ( int k = 0; k < 4; k++ ) {
+                    if ( k < n ) {
+                        if ( MOVE ) { pc[ base + k ] = c[k]; pxx[ base + k ] = x0[k]; pxy[ base + k ] = x1[k]; }
+                        if ( PUSH || rxl || rxu ) pux[ base + k ] = u0[k];
+                        if ( PUSH || ryl || ryu ) puy[ base + k ] = u1[k];
+                        if ( PUSH ) puz[ base + k ] = u2[k];
+                    }
+                }
+            }
+        }
+
+        if ( DETECT ) {
+            // warp-aggregated append of leaver indices (one global atomic per warp)
+            int nl = 0;
+#pragma unroll
+            for ( int k = 0; k < 4; k++ ) nl += ( leave_dir[k] != 4 );
+            const unsigned any = __ballot_sync( 0xffffffffu, nl > 0 );
+            if ( any ) {
+                int incl = nl;
+#pragma unroll
+                for ( int o = 1; o < 32; o <<= 1 ) {
+                    const int v = __shfl_up_sync( 0xffffffffu, incl, o );
+                    if ( lane >= o ) incl += v;
+                }
+                const int total = __shfl_sync( 0xffffffffu, incl, 31 );
+                int wbase = 0;
+                if ( lane == 31 ) wbase = atomicAdd( S.nidx + t, total );
+                wbase = __shfl_sync( 0xffffffffu, wbase, 31 );
+                int pos = wbase + incl - nl;
+#pragma unroll
+                for ( int k = 0; k < 4; k++ ) {
+                    if ( leave_dir[k] != 4 ) {
+                        S.idx[ off + pos ] = base + k;
+                        pos++;
+                        atomicAdd( S.npt + 9 * t + leave_dir[k], 1 );
+                    }
+                }
+            }
+        }
+    }
+
+    if ( PUSH ) {
+        // deterministic per-item energy: warp tree, then warps in order
+#pragma unroll
+        for ( int o = 16; o > 0; o >>= 1 ) energy += __shfl_down_sync( 0xffffffffu, energy, o );
+        if ( lane == 0 ) sred[ threadIdx.x >> 5 ] = energy;
+    }
+    __syncthreads();
+    if ( threadIdx.x == 0 ) {
+        if ( PUSH ) {
+            double e = 0.0;
+            for ( int w = 0; w < ( (int) blockDim.x >> 5 ); w++ ) e += sred[w];
+            S.energy[ eidx ] = e;
+        }
+        if ( MOVE && it.chunk == 0 ) atomicAdd( S.nmove, (unsigned long long) np );
+        if ( MOVE == 2 ) {
+            fence_proxy_async_smem();
+            bulk_s2g_add_f32( R.Jdep + (size_t) t * 3 * tv, sJ, 12u * tv );
+            bulk_commit();
+            bulk_wait_all();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tile sort (particles.cpp:212-614 semantics; slot layout with slack)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ int wrap_tile( int v, int n, int periodic ) {
+    if ( periodic ) { if ( v < 0 ) v += n; if ( v >= n ) v -= n; return v; }
+    return ( v >= 0 && v < n ) ? v : -1;
+}
+
+// Block-wide exclusive scan of one value per thread; the block total is
+// written to *total (a shared variable) and visible on return.
+template < int NT >
+__device__ __forceinline__ long long block_exscan( long long v, long long * total ) {
+    static_assert( NT % 32 == 0 && NT <= 1024, "block size" );
+    __shared__ long long wsum[ NT / 32 ];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long incl = v;
+#pragma unroll
+    for ( int o = 1; o < 32; o <<= 1 ) {
+        const long long y = __shfl_up_sync( 0xffffffffu, incl, o );
+        if ( lane >= o ) incl += y;
+    }
+    if ( lane == 31 ) wsum[w] = incl;
+    __syncthreads();
+    if ( w == 0 ) {
+        const long long s = ( lane < NT / 32 ) ? wsum[lane] : 0;
+        long long si = s;
+#pragma unroll
+        for ( int o = 1; o < 32; o <<= 1 ) {
+            const long long y = __shfl_up_sync( 0xffffffffu, si, o );
+            if ( lane >= o ) si += y;
+        }
+        if ( lane < NT / 32 ) wsum[lane] = si - s;
+        if ( lane == NT / 32 - 1 ) *total = si;
+    }
+    __syncthreads();
+    const long long r = wsum[w] + incl - v;
+    __syncthreads();
+    return r;
+}
+
+constexpr int PLAN_THREADS = 1024;
+
+// Sort plan: one CTA per species.  Counts incoming particles per tile,
+// decides between the in-place path (everything fits its slot and the
+// staging buffer) and a repack, and lays out offsets for either.
+__global__ void __launch_bounds__( PLAN_THREADS )
+k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_list,
+             const RunDev * __restrict__ runs, int use_extra )
+{
+    const SpDev & S = sps[ species_list[ blockIdx.x ] ];
+    const RunDev & R = runs[ S.run ];
+    const int nt = S.ntiles;
+    const int ntx = R.ntx, nty = R.nty;
+    const int per = ( nt + PLAN_THREADS - 1 ) / PLAN_THREADS;
+    const int t0 = min( nt, (int) threadIdx.x * per ), t1 = min( nt, t0 + per );
+    __shared__ long long s_total;
+    __shared__ int s_fit;
+    if ( threadIdx.x == 0 ) s_fit = 1;
+    __syncthreads();
+
+    long long in_sum = 0;
+    int fit = 1;
+    for ( int t = t0; t < t1; t++ ) {
+        const int tx = t % ntx, ty = t / ntx;
+        int in = 0;
+        for ( int d = 0; d < 9; d++ ) {
+            if ( d == 4 ) continue;
+            const int sx = wrap_tile( tx - ( d % 3 - 1 ), ntx, S.perx );
+            const int sy = wrap_tile( ty - ( d / 3 - 1 ), nty, S.pery );
+            if ( sx >= 0 && sy >= 0 ) in += S.npt[ 9 * ( sy * ntx + sx ) + d ];
+        }
+        const int stay = S.np[t] - S.nidx[t];
+        const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
+        S.in_cnt[t] = in;
+        S.new_np[t] = stay + in;
+        S.stage_cnt[t] = 0;
+        if ( stay + in + ex > S.cap[t] ) fit = 0;
+        in_sum += in;
+    }
+    if ( !fit ) s_fit = 0;
+    long long total;
+    long long pre = block_exscan< PLAN_THREADS >( in_sum, &s_total );
+    __syncthreads();
+    total = s_total;
+    for ( int t = t0; t < t1; t++ ) { S.stage_off[t] = (int) pre; pre += S.in_cnt[t]; }
+
+    const int repack = !s_fit || total > S.stage_cap;
+    if ( !repack ) {
+        if ( threadIdx.x == 0 ) {
+            *S.mode = 0;
+        }
+        return;
+    }
+    if ( threadIdx.x == 0 && total > S.stage_cap ) atomicOr( R.status, ST_STAGE_OVERFLOW );
+
+    // Repack layout: need[t] rounded up to 4, then the free capacity spread in
+    // proportion to need[t] + min_slack (multiples of 4).
+    long long need_sum = 0, w_sum = 0;
+    for ( int t = t0; t < t1; t++ ) {
+        const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
+        const int need = ( S.new_np[t] + ex + 3 ) & ~3;
+        need_sum += need;
+        w_sum += need + S.min_slack;
+    }
+    __syncthreads();
+    long long pre_need = block_exscan< PLAN_THREADS >( need_sum, &s_total );
+    __syncthreads();
+    const long long need_total = s_total;
+    __syncthreads();
+    (void) pre_need;
+    block_exscan< PLAN_THREADS >( w_sum, &s_total );
+    __syncthreads();
+    const long long w_total = s_total;
+    const long long free_cap = (long long) S.max_part - need_total;
+    if ( free_cap < 0 ) {
+        if ( threadIdx.x == 0 ) { *S.mode = 2; atomicOr( R.status, ST_CAPACITY ); }
+        return;
+    }
+    long long cap_sum = 0;
+    for ( int t = t0; t < t1; t++ ) {
+        const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
+        const int need = ( S.new_np[t] + ex + 3 ) & ~3;
+        const long long slack = w_total > 0 ? ( free_cap * ( need + S.min_slack ) ) / w_total : 0;
+        const int c = need + (int) ( slack & ~3LL );
+        S.new_cap[t] = c;
+        cap_sum += c;
+    }
+    __syncthreads();
+    long long pc = block_exscan< PLAN_THREADS >( cap_sum, &s_total );
+    for ( int t = t0; t < t1; t++ ) { S.new_off[t] = (int) pc; pc += S.new_cap[t]; }
+    if ( threadIdx.x == 0 ) *S.mode = 1;
+}
+
+__device__ __forceinline__ void copy_particle( const PartArrays & d, size_t di, const PartArrays & s, size_t si ) {
+    d.cell[di] = s.cell[si]; d.xx[di] = s.xx[si]; d.xy[di] = s.xy[si];
+    d.ux[di] = s.ux[si]; d.uy[di] = s.uy[si]; d.uz[di] = s.uz[si];
+}
+
+constexpr int SORT_THREADS = 128;
+
+// Leavers to staging (or, when repacking, every particle to buffer B), then
+// fill the holes left in [0, n0) with the stayers found in the tail.
+__global__ void __launch_bounds__( SORT_THREADS )
+k_sort_out( const Item * __restrict__ items, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs )
+{
+    const Item it = items[ blockIdx.x ];
+    const SpDev & S = sps[ it.sp ];
+    const RunDev & R = runs[ S.run ];
+    const int mode = *S.mode;
+    if ( mode == 2 ) return;
+    const int t = it.tile;
+    const int ntx = R.ntx, nty = R.nty, nxx = R.nxx, nxy = R.nxy;
+    const int tx = t % ntx, ty = t / ntx;
+    const int np = S.np[t], nl = S.nidx[t], n0 = np - nl, off = S.off[t];
+    __shared__ int s_nh, s_ns;
+    if ( threadIdx.x == 0 ) { s_nh = 0; s_ns = 0; }
+    __syncthreads();
+
+    if ( mode == 0 ) {
+        for ( int k = threadIdx.x; k < nl; k += blockDim.x ) {
+            const int i = S.idx[ off + k ];
+            const size_t g = (size_t) off + i;
+            const uint32_t c = S.A.cell[g];
+            int ix = cell_x( c ), iy = cell_y( c );
+            const int xc = ( ix >= nxx ) - ( ix < 0 ), yc = ( iy >= nxy ) - ( iy < 0 );
+            const int ttx = wrap_tile( tx + xc, ntx, S.perx ), tty = wrap_tile( ty + yc, nty, S.pery );
+            if ( ttx >= 0 && tty >= 0 ) {
+                const int tt = tty * ntx + ttx;
+                const int slot = atomicAdd( S.stage_cnt + tt, 1 );
+                const size_t d = (size_t) S.stage_off[tt] + slot;
+                S.S.cell[d] = pack_cell( ix - xc * nxx, iy - yc * nxy );
+                S.S.xx[d] = S.A.xx[g]; S.S.xy[d] = S.A.xy[g];
+                S.S.ux[d] = S.A.ux[g]; S.S.uy[d] = S.A.uy[g]; S.S.uz[d] = S.A.uz[g];
+            }
+            if ( i < n0 ) S.aux[ off + atomicAdd( &s_nh, 1 ) ] = i;
+        }
+        for ( int ci = n0 + threadIdx.x; ci < np; ci += blockDim.x ) {
+            const uint32_t c = S.A.cell[ (size_t) off + ci ];
+            const int ix = cell_x( c ), iy = cell_y( c );
+            if ( ix >= 0 && ix < nxx && iy >= 0 && iy < nxy ) S.aux2[ off + atomicAdd( &s_ns, 1 ) ] = ci;
+        }
+        __syncthreads();
+        const int nh = min( s_nh, s_ns );
+        if ( threadIdx.x == 0 && s_nh != s_ns ) atomicOr( R.status, ST_BAD_CELL );
+        for ( int r = threadIdx.x; r < nh; r += blockDim.x )
+            copy_particle( S.A, (size_t) off + S.aux[ off + r ], S.A, (size_t) off + S.aux2[ off + r ] );
+        __syncthreads();
+        if ( threadIdx.x == 0 ) S.np[t] = n0;
+    } else {
+        // repack: stayers to B at new_off[t] + rank, leavers to B after the
+        // target's stayers.
+        for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
+            const size_t g = (size_t) off + i;
+            const uint32_t c = S.A.cell[g];
+            const int ix = cell_x( c ), iy = cell_y( c );
+            const int xc = ( ix >= nxx ) - ( ix < 0 ), yc = ( iy >= nxy ) - ( iy < 0 );
+            if ( xc == 0 && yc == 0 ) {
+                const size_t d = (size_t) S.new_off[t] + atomicAdd( &s_ns, 1 );
+                copy_particle( S.B, d, S.A, g );
+            } else {
+                const int ttx = wrap_tile( tx + xc, ntx, S.perx ), tty = wrap_tile( ty + yc, nty, S.pery );
+                if ( ttx >= 0 && tty >= 0 ) {
+                    const int tt = tty * ntx + ttx;
+                    const int slot = atomicAdd( S.stage_cnt + tt, 1 );
+                    const size_t d = (size_t) S.new_off[tt] + ( S.np[tt] - S.nidx[tt] ) + slot;
+                    copy_particle( S.B, d, S.A, g );
+                    S.B.cell[d] = pack_cell( ix - xc * nxx, iy - yc * nxy );
+                }
+            }
+        }
+    }
+}
+
+// Incoming particles from staging appended after the stayers (or the
+// repacked tile copied back from B); resets the per-tile leaver counters.
+__global__ void __launch_bounds__( SORT_THREADS )
+k_sort_in( const Item * __restrict__ items, const SpDev * __restrict__ sps )
+{
+    const Item it = items[ blockIdx.x ];
+    const SpDev & S = sps[ it.sp ];
+    const int mode = *S.mode;
+    const int t = it.tile;
+    if ( mode == 0 ) {
+        const int n0 = S.np[t], in = S.in_cnt[t], off = S.off[t], so = S.stage_off[t];
+        for ( int k = threadIdx.x; k < in; k += blockDim.x )
+            copy_particle( S.A, (size_t) off + n0 + k, S.S, (size_t) so + k );
+        __syncthreads();
+        if ( threadIdx.x == 0 ) S.np[t] = n0 + in;
+    } else if ( mode == 1 ) {
+        const int n = S.new_np[t], off = S.new_off[t];
+        for ( int k = threadIdx.x; k < n; k += blockDim.x )
+            copy_particle( S.A, (size_t) off + k, S.B, (size_t) off + k );
+        __syncthreads();
+        if ( threadIdx.x == 0 ) { S.np[t] = n; S.off[t] = off; S.cap[t] = S.new_cap[t]; }
+    }
+    if ( threadIdx.x < 9 ) S.npt[ 9 * t + threadIdx.x ] = 0;
+    if ( threadIdx.x == 0 ) S.nidx[t] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Injection (density.cpp): particles of a cell range appended to each tile.
+// The order of the reference's sequential loops (i1, i0, cell) is kept with
+// a block-wide ordered scan.
+// ---------------------------------------------------------------------------
+struct InjRule {
+    int type;                 // 1 uniform, 2 step, 3 slab, 4 sphere
+    int diry;
+    float a, b;               // step pos / slab begin,end (cells)
+    float cx, cy, r2;         // sphere (simulation units)
+    float dxx, dxy;
+    int ppcx, ppcy;
+    int range[4];             // x.lower, x.upper, y.lower, y.upper (global cells)
+    int tx_limit;             // tiles processed along x (reference quirk for dir = y)
+};
+
+__device__ __forceinline__ int inj_test( const InjRule & r, int shiftx, int shifty, int cx, int cy, float posx, float posy ) {
+    float t;
+    switch ( r.type ) {
+    case 1: return 1;
+    case 2:
+        t = r.diry ? (float) ( ( shifty + cy ) + ( (double) posy + 0.5 ) ) : (float) ( ( shiftx + cx ) + ( (double) posx + 0.5 ) );
+        return t > r.a;
+    case 3:
+        t = r.diry ? (float) ( ( shifty + cy ) + ( (double) posy + 0.5 ) ) : (float) ( ( shiftx + cx ) + ( (double) posx + 0.5 ) );
+        return ( t >= r.a ) && ( t < r.b );
+    case 4: {
+        const float gx = (float) ( ( ( shiftx + cx ) + ( (double) posx + 0.5 ) ) * (double) r.dxx );
+        const float gy = (float) ( ( ( shifty + cy ) + ( (double) posy + 0.5 ) ) * (double) r.dxy );
+        return ( gx - r.cx ) * ( gx - r.cx ) + ( gy - r.cy ) * ( gy - r.cy ) < r.r2;
+    }
+    }
+    return 0;
+}
+
+__device__ __forceinline__ bool inj_tile_range( const InjRule & r, int tx, int ty, int nxx, int nxy,
+                                                int & ri0, int & ri1, int & rj0, int & rj1 ) {
+    ri0 = r.range[0] - tx * nxx; ri1 = r.range[1] - tx * nxx;
+    rj0 = r.range[2] - ty * nxy; rj1 = r.range[3] - ty * nxy;
+    if ( ( ri0 < nxx ) && ( ri1 >= 0 ) && ( rj0 < nxy ) && ( rj1 >= 0 ) ) {
+        if ( ri0 < 0 ) ri0 = 0;
+        if ( rj0 < 0 ) rj0 = 0;
+        if ( ri1 >= nxx ) ri1 = nxx - 1;
+        if ( rj1 >= nxy ) rj1 = nxy - 1;
+        return true;
+    }
+    return false;
+}
+
+constexpr int INJ_THREADS = 256;
+
+// count == 1: write the number of particles to inject per tile to S.extra
+// count == 0: inject them after the existing particles of each tile
+__global__ void __launch_bounds__( INJ_THREADS )
+k_inject( int sp, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs, InjRule r, int count )
+{
+    const SpDev & S = sps[sp];
+    const RunDev & R = runs[ S.run ];
+    const int t = blockIdx.x;
+    const int tx = t % R.ntx, ty = t / R.ntx;
+    const int nxx = R.nxx, nxy = R.nxy;
+    int ri0, ri1, rj0, rj1;
+    const bool in_range = ( tx < r.tx_limit ) && inj_tile_range( r, tx, ty, nxx, nxy, ri0, ri1, rj0, rj1 );
+    if ( !in_range ) {
+        if ( count && threadIdx.x == 0 ) S.extra[t] = 0;
+        return;
+    }
+    const int row = ri1 - ri0 + 1, vol = ( rj1 - rj0 + 1 ) * row;
+    const int total = vol * r.ppcx * r.ppcy;
+    const int shiftx = tx * nxx, shifty = ty * nxy;
+    const double dpcx = 1.0 / r.ppcx, dpcy = 1.0 / r.ppcy;
+    __shared__ long long s_tot;
+    int run = 0;
+    const int base = count ? 0 : S.np[t];
+    const int off = S.off[t];
+    for ( int L0 = 0; L0 < total; L0 += INJ_THREADS ) {
+        const int L = L0 + threadIdx.x;
+        int inj = 0, cx = 0, cy = 0; float posx = 0, posy = 0;
+        if ( L < total ) {
+            const int idx = L % vol, pidx = L / vol;
+            const int i0 = pidx % r.ppcx, i1 = pidx / r.ppcx;
+            posx = (float) ( dpcx * ( i0 + 0.5 ) - 0.5 );
+            posy = (float) ( dpcy * ( i1 + 0.5 ) - 0.5 );
+            cx = idx % row + ri0; cy = idx / row + rj0;
+            inj = inj_test( r, shiftx, shifty, cx, cy, posx, posy );
+        }
+        long long pre = block_exscan< INJ_THREADS >( inj, &s_tot );
+        __syncthreads();
+        const int tot = (int) s_tot;
+        if ( !count && inj ) {
+            const size_t g = (size_t) off + base + run + pre;
+            S.A.cell[g] = pack_cell( cx, cy );
+            S.A.xx[g] = posx; S.A.xy[g] = posy;
+            S.A.ux[g] = 0.f; S.A.uy[g] = 0.f; S.A.uz[g] = 0.f;
+        }
+        run += tot;
+        __syncthreads();
+    }
+    if ( threadIdx.x == 0 ) {
+        if ( count ) S.extra[t] = run;
+        else S.np[t] = base + run;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Conversion between the slot layout and the reference's packed layout
+// (ix int2, x float2, u float3; tiles contiguous at packed offsets).
+// ---------------------------------------------------------------------------
+__global__ void k_pack( int sp, const SpDev * __restrict__ sps, const int * __restrict__ poff,
+                        int2 * __restrict__ ix, float2 * __restrict__ x, float * __restrict__ u )
+{
+    const SpDev & S = sps[sp];
+    const int t = blockIdx.x;
+    const int np = S.np[t], off = S.off[t], po = poff[t];
+    for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
+        const size_t g = (size_t) off + i, d = (size_t) po + i;
+        const uint32_t c = S.A.cell[g];
+        ix[d] = make_int2( cell_x( c ), cell_y( c ) );
+        x[d] = make_float2( S.A.xx[g], S.A.xy[g] );
+        u[3*d] = S.A.ux[g]; u[3*d+1] = S.A.uy[g]; u[3*d+2] = S.A.uz[g];
+    }
+}
+
+__global__ void k_unpack( int sp, const SpDev * __restrict__ sps, const int * __restrict__ poff,
+                          const int2 * __restrict__ ix, const float2 * __restrict__ x, const float * __restrict__ u )
+{
+    const SpDev & S = sps[sp];
+    const int t = blockIdx.x;
+    const int np = S.np[t], off = S.off[t], po = poff[t];
+    for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
+        const size_t g = (size_t) off + i, s = (size_t) po + i;
+        S.A.cell[g] = pack_cell( ix[s].x, ix[s].y );
+        S.A.xx[g] = x[s].x; S.A.xy[g] = x[s].y;
+        S.A.ux[g] = u[3*s]; S.A.uy[g] = u[3*s+1]; S.A.uz[g] = u[3*s+2];
+    }
+}
+
+// Species::gather (particles.cpp:16-200): value per particle at packed offsets,
+// optionally scaled as fma(scale.x, val, scale.y).
+__global__ void k_gather( int sp, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs,
+                          const int * __restrict__ poff, int quant, float sx, float sy, int scaled,
+                          float * __restrict__ out )
+{
+    const SpDev & S = sps[sp];
+    const RunDev & R = runs[ S.run ];
+    const int t = blockIdx.x;
+    const int tx = t % R.ntx, ty = t / R.ntx;
+    const int np = S.np[t], off = S.off[t], po = poff[t];
+    for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
+        const size_t g = (size_t) off + i;
+        float val;
+        switch ( quant ) {
+        case 0: val = ( tx * R.nxx + cell_x( S.A.cell[g] ) ) + ( 0.5f + S.A.xx[g] ); break;
+        case 1: val = ( ty * R.nxy + cell_y( S.A.cell[g] ) ) + ( 0.5f + S.A.xy[g] ); break;
+        case 2: val = S.A.ux[g]; break;
+        case 3: val = S.A.uy[g]; break;
+        default: val = S.A.uz[g]; break;
+        }
+        out[ (size_t) po + i ] = scaled ? __fmaf_rn( sx, val, sy ) : val;
+    }
+}
+
+// Charge deposit (species.cpp:2348-2399) into a tiled scalar grid with guard
+// cells {0,1}; per-tile shared-memory accumulation, then a store of the tile.
+__global__ void k_dep_charge( int sp, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs,
+                              float * __restrict__ charge, int cextx, int cvol )
+{
+    extern __shared__ float sc[];
+    const SpDev & S = sps[sp];
+    const int t = blockIdx.x;
+    for ( int i = threadIdx.x; i < cvol; i += blockDim.x ) sc[i] = 0.f;
+    __syncthreads();
+    const int np = S.np[t], off = S.off[t];
+    const float q = S.q;
+    for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
+        const size_t g = (size_t) off + i;
+        const uint32_t c = S.A.cell[g];
+        const int idx = cell_y( c ) * cextx + cell_x( c );
+        const float xx = S.A.xx[g], xy = S.A.xy[g];
+        const float s0x = 0.5f - xx, s1x = 0.5f + xx, s0y = 0.5f - xy, s1y = 0.5f + xy;
+        atomicAdd( sc + idx, s0y * s0x * q );
+        atomicAdd( sc + idx + 1, s0y * s1x * q );
+        atomicAdd( sc + idx + cextx, s1y * s0x * q );
+        atomicAdd( sc + idx + 1 + cextx, s1y * s1x * q );
+    }
+    __syncthreads();
+    for ( int i = threadIdx.x; i < cvol; i += blockDim.x ) charge[ (size_t) t * cvol + i ] += sc[i];
+    (void) runs;
+}
+
+// Per-item energy sums reduced per species in item order (deterministic).
+__global__ void k_energy_sum( const SpDev * __restrict__ sps, int sp, int nitems, double * __restrict__ out )
+{
+    const SpDev & S = sps[sp];
+    __shared__ double s[256];
+    double a = 0.0;
+    const int per = ( nitems + blockDim.x - 1 ) / blockDim.x;
+    const int i0 = threadIdx.x * per, i1 = min( nitems, i0 + per );
+    for ( int i = i0; i < i1; i++ ) a += S.energy[i];
+    s[ threadIdx.x ] = a;
+    __syncthreads();
+    if ( threadIdx.x == 0 ) {
+        double tot = 0.0;
+        for ( int i = 0; i < (int) blockDim.x; i++ ) tot += s[i];
+        *out = tot;
+    }
+}
+
+// Tile counts: np_total and np_max_tile
+__global__ void k_np_stats( const SpDev * __restrict__ sps, int sp, unsigned long long * __restrict__ out )
+{
+    const SpDev & S = sps[sp];
+    __shared__ unsigned long long s_sum[256];
+    __shared__ unsigned s_max[256];
+    unsigned long long a = 0; unsigned m = 0;
+    for ( int t = threadIdx.x; t < S.ntiles; t += blockDim.x ) { a += S.np[t]; m = max( m, (unsigned) S.np[t] ); }
+    s_sum[ threadIdx.x ] = a; s_max[ threadIdx.x ] = m;
+    __syncthreads();
+    if ( threadIdx.x == 0 ) {
+        unsigned long long tot = 0; unsigned mx = 0;
+        for ( int i = 0; i < (int) blockDim.x; i++ ) { tot += s_sum[i]; mx = max( mx, s_max[i] ); }
+        out[0] = tot; out[1] = mx;
+    }
+}
+
+}  // namespace zb
+
+// ---------------------------------------------------------------------------
+// Launch wrappers (host side of this translation unit)
+// ---------------------------------------------------------------------------
+namespace zb {
+
+size_t particle_smem_bytes( int tile_vol ) {
+    return (size_t) 3 * 3 * tile_vol * sizeof( float ) + 16 + 32 * sizeof( double );
+}
+
+typedef void ( *pk_fn )( const Item *, const SpDev *, const RunDev *, const int * );
+
+static pk_fn pick_particle_kernel( int push, int move, int detect ) {
+#define PK( P, M, D ) if ( push == P && move == M && detect == D ) return k_particles< P, M, D >;
+    PK( 1, 2, true ) PK( 2, 2, true )
+    PK( 1, 0, false ) PK( 2, 0, false )
+    PK( 0, 2, true ) PK( 0, 1, true ) PK( 0, 0, true )
+    PK( 1, 1, true ) PK( 2, 1, true )
+#undef PK
+    return nullptr;
+}
+
+cudaError_t launch_particles( cudaStream_t st, int push, int move, int detect, const Item * items, int nitems,
+                              const SpDev * sps, const RunDev * runs, const int * shifts, int max_tile_vol ) {
+    pk_fn f = pick_particle_kernel( push, move, detect );
+    if ( !f ) return cudaErrorInvalidValue;
+    const size_t smem = particle_smem_bytes( max_tile_vol );
+    if ( smem > 48 * 1024 )
+        cudaFuncSetAttribute( (const void *) f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
+    if ( nitems <= 0 ) return cudaSuccess;
+    f<<< nitems, PK_THREADS, smem, st >>>( items, sps, runs, shifts );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort( cudaStream_t st, const Item * items, int nitems, const SpDev * sps,
+                         const int * species_list, int nspecies, const RunDev * runs, int use_extra ) {
+    if ( nitems <= 0 ) return cudaSuccess;
+    k_sort_plan<<< nspecies, PLAN_THREADS, 0, st >>>( sps, species_list, runs, use_extra );
+    k_sort_out<<< nitems, SORT_THREADS, 0, st >>>( items, sps, runs );
+    k_sort_in<<< nitems, SORT_THREADS, 0, st >>>( items, sps );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_inject( cudaStream_t st, int sp, int ntiles, const SpDev * sps, const RunDev * runs,
+                           const InjRule & r, int count ) {
+    k_inject<<< ntiles, INJ_THREADS, 0, st >>>( sp, sps, runs, r, count );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack( cudaStream_t st, int sp, int ntiles, const SpDev * sps, const int * poff,
+                         int2 * ix, float2 * x, float * u ) {
+    k_pack<<< ntiles, 256, 0, st >>>( sp, sps, poff, ix, x, u );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack( cudaStream_t st, int sp, int ntiles, const SpDev * sps, const int * poff,
+                           const int2 * ix, const float2 * x, const float * u ) {
+    k_unpack<<< ntiles, 256, 0, st >>>( sp, sps, poff, ix, x, u );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather( cudaStream_t st, int sp, int ntiles, const SpDev * sps, const RunDev * runs,
+                           const int * poff, int quant, float sx, float sy, int scaled, float * out ) {
+    k_gather<<< ntiles, 256, 0, st >>>( sp, sps, runs, poff, quant, sx, sy, scaled, out );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dep_charge( cudaStream_t st, int sp, int ntiles, const SpDev * sps, const RunDev * runs,
+                               float * charge, int cextx, int cvol ) {
+    k_dep_charge<<< ntiles, 256, cvol * sizeof( float ), st >>>( sp, sps, runs, charge, cextx, cvol );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy_sum( cudaStream_t st, const SpDev * sps, int sp, int nitems, double * out ) {
+    k_energy_sum<<< 1, 256, 0, st >>>( sps, sp, nitems, out );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_np_stats( cudaStream_t st, const SpDev * sps, int sp, unsigned long long * out ) {
+    k_np_stats<<< 1, 256, 0, st >>>( sps, sp, out );
+    return cudaGetLastError();
+}
+
+}  // namespace zb

@@ -1,0 +1,169 @@
+// zpic_dev.cuh -- device-side descriptors and helpers shared by the em2d kernels.
+//
+// Data layout in HBM
+//   fields  : per-tile float3 blocks with guard cells {1,2} on both axes, the
+//             reference's tiled layout (grid.h:77-92): tile_vol =
+//             roundup4(ext_x*ext_y) cells per tile, cell (0,0) at gc_off.
+//   particles: six SoA arrays per species, one slot per tile
+//             [off[t], off[t]+cap[t]) with np[t] used entries; off[] and cap[]
+//             are multiples of 4 so a thread loads 4 particles with 128-bit
+//             accesses.  cell = (int16 ix.x) | (int16 ix.y) << 16.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace zb {
+
+// Status bits written by kernels (host reads them after synchronising).
+enum : int {
+    ST_WAIT_TIMEOUT   = 1,    // a bounded mbarrier / bulk-copy wait gave up
+    ST_STAGE_OVERFLOW = 2,    // sort staging buffer too small (repack taken)
+    ST_CAPACITY       = 4,    // particle buffer too small for the new layout
+    ST_BAD_CELL       = 8,    // a particle moved more than one tile (invalid input)
+};
+
+// Per-simulation (run) geometry and field buffers.
+struct RunDev {
+    int ntx, nty, nxx, nxy;       // tiles, tile size
+    int extx, exty;               // tile size with guard cells
+    int gc_off;                   // offset of cell (0,0) inside a tile block
+    int tile_vol;                 // cells per tile block
+    float * E; float * B;         // float3 per cell
+    float * J;                    // final current (after guard-cell exchange)
+    float * Jdep;                 // raw deposits (tile-local sums incl. guard cells)
+    int emf_perx, emf_pery;       // E/B periodic flags (grid::periodic)
+    int cur_perx, cur_pery;       // J periodic flags
+    float dtx, dty, dtx2, dty2;   // Yee coefficients dt/dx, dt/dy and halves (emf.cpp:524-525)
+    float dt;                     // dt as passed to yeeJ_e (FP32)
+    int emf_bc[4];                // emf::bc
+    int cur_bc[4];                // current::bc
+    int * status;                 // ST_* bits
+};
+
+// Particle arrays of one buffer (A, repack buffer B or staging).
+struct PartArrays {
+    uint32_t * cell;
+    float * xx; float * xy;
+    float * ux; float * uy; float * uz;
+};
+
+// Per-species state.
+struct SpDev {
+    int run;
+    int ntiles;
+    int nchunk;                   // CTAs per tile in the particle kernel
+    int max_part;                 // capacity of A and B
+    int stage_cap;                // capacity of the staging buffer
+    PartArrays A, B, S;
+    int * np; int * off; int * cap;          // tile slots of A
+    int * npt;                    // [ntiles*9] leavers per direction (npt[4] unused)
+    int * nidx;                   // [ntiles] leavers per tile
+    int * idx;                    // [max_part] local index of leavers, at off[t]+k
+    int * aux; int * aux2;        // [max_part] hole / tail lists, at off[t]+k
+    int * in_cnt;                 // [ntiles] incoming particles
+    int * stage_off;              // [ntiles] staging offsets (exclusive scan of in_cnt)
+    int * stage_cnt;              // [ntiles] staging fill counters
+    int * new_off; int * new_cap; int * new_np;  // [ntiles] repack layout
+    int * extra;                  // [ntiles] room to reserve for injection (or nullptr)
+    int * mode;                   // [1] 0 = in-place sort, 1 = repack
+    double * energy;              // [ntiles*nchunk] per work-item kinetic energy sums
+    unsigned long long * nmove;   // pushes counter
+    float alpha;                  // 0.5*dt/m_q (species.cpp:2305)
+    float dt_dx, dt_dy;           // dt/dx (species.cpp:2140-2143)
+    float q;                      // charge per particle
+    float qnx, qny;               // q*dx/dt (species.cpp:2145-2148)
+    int perx, pery;               // particle periodic flags
+    int bc[4];                    // species::bc
+    int min_slack;                // minimum free slots per tile after a repack
+};
+
+// ---------------------------------------------------------------------------
+// PTX helpers: bulk asynchronous copies (TMA, non-tensor form) and mbarriers.
+// No multicast forms are used anywhere.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32( const void * p ) {
+    return static_cast<uint32_t>( __cvta_generic_to_shared( p ) );
+}
+
+__device__ __forceinline__ void mbar_init( uint64_t * bar, uint32_t count ) {
+    asm volatile( "mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"( smem_u32( bar ) ), "r"( count ) : "memory" );
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile( "fence.proxy.async.shared::cta;" ::: "memory" );
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx( uint64_t * bar, uint32_t bytes ) {
+    asm volatile( "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                  :: "r"( smem_u32( bar ) ), "r"( bytes ) : "memory" );
+}
+
+__device__ __forceinline__ bool mbar_try_wait_parity( uint64_t * bar, uint32_t parity ) {
+    uint32_t ok;
+    asm volatile( "{\n\t.reg .pred p;\n\t"
+                  "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                  "selp.u32 %0, 1, 0, p;\n\t}"
+                  : "=r"( ok ) : "r"( smem_u32( bar ) ), "r"( parity ) : "memory" );
+    return ok != 0;
+}
+
+// Global -> shared bulk copy completing on an mbarrier.  dst, src 16-byte
+// aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s( void * dst, const void * src, uint32_t bytes, uint64_t * bar ) {
+    asm volatile( "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                  :: "r"( smem_u32( dst ) ), "l"( src ), "r"( bytes ), "r"( smem_u32( bar ) ) : "memory" );
+}
+
+// Shared -> global bulk copy (bulk-group completion).
+__device__ __forceinline__ void bulk_s2g( void * dst, const void * src, uint32_t bytes ) {
+    asm volatile( "cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                  :: "l"( dst ), "r"( smem_u32( src ) ), "r"( bytes ) : "memory" );
+}
+
+// Shared -> global bulk element-wise reduction: dst[i] += src[i] (f32, atomic per element).
+__device__ __forceinline__ void bulk_s2g_add_f32( float * dst, const float * src, uint32_t bytes ) {
+    asm volatile( "cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f32 [%0], [%1], %2;"
+                  :: "l"( dst ), "r"( smem_u32( src ) ), "r"( bytes ) : "memory" );
+}
+
+__device__ __forceinline__ void bulk_commit() {
+    asm volatile( "cp.async.bulk.commit_group;" ::: "memory" );
+}
+
+// Wait until the shared-memory sources of all committed bulk groups have been read.
+__device__ __forceinline__ void bulk_wait_read_all() {
+    asm volatile( "cp.async.bulk.wait_group.read 0;" ::: "memory" );
+}
+
+// Wait until all committed bulk groups are complete (writes visible).
+__device__ __forceinline__ void bulk_wait_all() {
+    asm volatile( "cp.async.bulk.wait_group 0;" ::: "memory" );
+}
+
+// Bounded wait on an mbarrier phase.  Gives up after ~0.5 s, records
+// ST_WAIT_TIMEOUT and returns false; never traps.
+__device__ __forceinline__ bool mbar_wait_bounded( uint64_t * bar, uint32_t parity, int * status ) {
+    for ( int i = 0; i < ( 1 << 22 ); i++ ) {
+        if ( mbar_try_wait_parity( bar, parity ) ) return true;
+        if ( i > 16 ) __nanosleep( 128 );
+    }
+    atomicOr( status, ST_WAIT_TIMEOUT );
+    return false;
+}
+
+// Tile-local cell index packing
+__device__ __forceinline__ uint32_t pack_cell( int ix, int iy ) {
+    return ( static_cast<uint32_t>( ix ) & 0xFFFFu ) | ( static_cast<uint32_t>( iy ) << 16 );
+}
+__device__ __forceinline__ int cell_x( uint32_t c ) { return static_cast<int>( static_cast<int16_t>( c & 0xFFFFu ) ); }
+__device__ __forceinline__ int cell_y( uint32_t c ) { return static_cast<int>( static_cast<int16_t>( c >> 16 ) ); }
+
+// Work item of the particle kernels: species, tile, chunk
+struct Item { int sp; int tile; int chunk; int pad; };
+
+}  // namespace zb
