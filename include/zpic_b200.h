@@ -206,6 +206,29 @@ int zpic_b200_grid_set( zpic_sim * sim, int32_t which, const float * in );
 /* vec3grid::gather (vec3grid.h:76-205): one component, dense [ny][nx] */
 int zpic_b200_grid_gather( zpic_sim * sim, int32_t which, int32_t fc, float * out );
 
+/*
+ * ---- charge density without device allocation ----
+ * No counterpart in the reference.  Same result as zpic_b200_species_charge
+ * (dense [ny][nx] charge density of one particle set), for callers that
+ * cannot allocate device memory: frameworks that own all device memory
+ * through their own pool, allocation-free real-time / in-situ loops, and
+ * code recorded into CUDA graphs (cudaMalloc cannot be captured).
+ * The caller passes device pointers: per-tile particle counts and offsets of
+ * a packed particle set (the layout zpic_b200_species_get returns: ix as
+ * 2 int32, x as 2 float per particle), the charge per particle q, and the
+ * output grid of ntiles_x*nx_x * ntiles_y*nx_y floats; work is queued on
+ * `stream` (a cudaStream_t, or NULL for the default stream).
+ * Scratch lives in a fixed 32 MiB device array owned by the library (held on
+ * every GPU that loads it until exit): ntiles * roundup4((nx_x+1)*(nx_y+1))
+ * must not exceed 8 Mi floats, larger grids are rejected with ZPIC_E_INVALID.
+ * The first call on a device resolves the array's address on that device;
+ * make that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised.
+ */
+int zpic_b200_charge_deposit_noalloc( uint32_t ntiles_x, uint32_t ntiles_y, uint32_t nx_x, uint32_t nx_y,
+                                      float q, const int32_t * np, const int32_t * offset,
+                                      const int32_t * ix, const float * x, float * charge, void * stream );
+
 /* ---- batched ensembles (no reference counterpart: many independent runs per launch) ---- */
 int zpic_b200_batch_create( zpic_sim * const * sims, int32_t n, zpic_batch ** out );
 int zpic_b200_batch_advance( zpic_batch * batch, int32_t nsteps );

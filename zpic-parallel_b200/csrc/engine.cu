@@ -60,6 +60,11 @@ static thread_local int g_device = -1;
 
 static int fail( int code, const std::string & msg ) { g_err = msg; return code; }
 
+namespace zb {
+// Sets the message zpic_b200_last_error() returns (for entry points in other files).
+void set_last_error( const std::string & msg ) { g_err = msg; }
+}
+
 #define CK( call )                                                                              \
     do {                                                                                        \
         cudaError_t e_ = ( call );                                                              \

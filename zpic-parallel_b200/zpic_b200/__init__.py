@@ -50,7 +50,7 @@ EXPORTS = [
     'zpic_b200_species_gather', 'zpic_b200_species_charge',
     'zpic_b200_grid_size', 'zpic_b200_grid_get', 'zpic_b200_grid_set', 'zpic_b200_grid_gather',
     'zpic_b200_batch_create', 'zpic_b200_batch_advance', 'zpic_b200_batch_synchronize',
-    'zpic_b200_batch_destroy',
+    'zpic_b200_batch_destroy', 'zpic_b200_charge_deposit_noalloc',
 ]
 
 
@@ -147,6 +147,7 @@ def lib():
             'zpic_b200_batch_advance': (I, [P, I]),
             'zpic_b200_batch_synchronize': (I, [P]),
             'zpic_b200_batch_destroy': (I, [P]),
+            'zpic_b200_charge_deposit_noalloc': (I, [U, U, U, U, ctypes.c_float, P, P, P, P, P, P]),
         }
         for name, (r, a) in sig.items():
             f = getattr(L, name)
@@ -449,6 +450,15 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def charge_deposit_noalloc(ntiles, nx, q, d_np, d_offset, d_ix, d_x, d_charge, stream=0):
+    """Charge density of a packed particle set already on the device, without
+    device allocation (see zpic_b200_charge_deposit_noalloc in include/zpic_b200.h).
+    Pointer arguments are device addresses (ints); raises ZpicError on failure."""
+    _check(lib().zpic_b200_charge_deposit_noalloc(
+        int(ntiles[0]), int(ntiles[1]), int(nx[0]), int(nx[1]), float(q),
+        d_np, d_offset, d_ix, d_x, d_charge, stream or None))
 
 
 def weibel_setup(sim, literal=False):
