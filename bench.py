@@ -12,8 +12,8 @@ as Simulation::get_nmove counts them, divided by the step time).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 With N > 1 (launched by torchrun) every rank runs its own replica of the
-workload (the path does not shard) and the timing is the
-maximum over ranks.  ``--impl reference`` times the reference's own OpenMP
+workload (a single run is not decomposed across GPUs; ensembles shard by
+run) and the timing is the maximum over ranks.  ``--impl reference`` times the reference's own OpenMP
 build (oracle/_ref, AVX2 variant) on the host cores instead.
 """
 import argparse
@@ -336,8 +336,121 @@ def run_gpu(args, world, rank, local):
     return 0
 
 
+def ensemble_specs(nruns, seed=0):
+    """Batched Weibel ensemble: grid N x N with N in {64,...,512}, ppc in
+    {2x2, 4x4, 8x8}, |ufl_z| ~ U[0.2, 0.8], uth ~ U[0.02, 0.15], drawn from a
+    seeded PCG64 generator."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    sizes = [64, 96, 128, 192, 256, 384, 512]
+    out = []
+    for _ in range(nruns):
+        n = int(rng.choice(sizes))
+        p = int(rng.choice([2, 4, 8]))
+        uz = float(rng.uniform(0.2, 0.8))
+        uth = float(rng.uniform(0.02, 0.15))
+        out.append((n, p, uz, uth))
+    return out
+
+
+def run_ensemble(args, world, rank, local):
+    """Weibel ensemble: many independent runs advanced together (one launch
+    per phase over all runs, CUDA-graph replay) vs the same runs each advanced
+    through its own graph, one after another and all at once on separate
+    streams.  Metric: aggregate run-steps per second, timed on the device."""
+    import torch
+    import zpic_b200 as zb
+    torch.cuda.set_device(local)
+    specs = ensemble_specs(args.runs)
+    specs = specs[rank::world]                  # runs shard across ranks, no exchange
+    sims = []
+    for n, p, uz, uth in specs:
+        s = zb.Simulation((n // TILE, n // TILE), (TILE, TILE), (n * DX, n * DX), DT, device=local)
+        s.add_species(-1.0, (p, p), udist=('thermalcorr', (uth, uth, uth), (0, 0, uz)))
+        s.add_species(1.0, (p, p), udist=('thermalcorr', (uth, uth, uth), (0, 0, -uz)))
+        sims.append(s)
+    nparticles = sum(s.np_total(0) + s.np_total(1) for s in sims)
+    batch = zb.Batch(sims)
+    # device timing: events on one stream that every participating stream
+    # joins before and after the timed region
+    clock = torch.cuda.Stream()
+    bstream = torch.cuda.ExternalStream(batch.stream_handle())
+    sstreams = [torch.cuda.ExternalStream(s.stream_handle()) for s in sims]
+
+    def timed(streams, work):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(clock)
+        for st in streams:
+            st.wait_event(ev0)
+        work()
+        for st in streams:
+            e = torch.cuda.Event()
+            e.record(st)
+            clock.wait_event(e)
+        ev1.record(clock)
+        torch.cuda.synchronize()
+        return max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, world)
+
+    batch.advance(args.warmup)
+    batch.synchronize()
+    l0 = batch.launch_count()
+    tb = timed([bstream], lambda: batch.advance(args.steps))
+    batch.synchronize()
+    launches = batch.launch_count() - l0
+    # plain: each run advanced on its own through its own CUDA graph, the runs
+    # one after another on the device (a sweep run by run) ...
+    for s in sims:
+        s.advance(args.warmup)
+    for s in sims:
+        s.synchronize()
+
+    def serial():
+        prev = None
+        for s, st in zip(sims, sstreams):
+            if prev is not None:
+                st.wait_event(prev)
+            s.advance(args.steps)
+            prev = torch.cuda.Event()
+            prev.record(st)
+    tp = timed(sstreams, serial)
+    for s in sims:
+        s.synchronize()
+
+    # ... and all runs issued at once on their own streams
+    def concurrent():
+        for s in sims:
+            s.advance(args.steps)
+    tc = timed(sstreams, concurrent)
+    for s in sims:
+        s.synchronize()
+    if rank == 0:
+        print(json.dumps({
+            'metric': 'ensemble_run_steps_per_second', 'value': args.runs * args.steps / tb,
+            'unit': 'run-steps/s', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': tb / args.steps * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded)',
+            'config': {'workload': 'Weibel ensemble, %d runs (seeded PCG64 draw of N, ppc, ufl, uth)' % args.runs,
+                       'particles_per_rank': nparticles, 'runs_per_rank': len(sims)},
+            'plain': {'value': args.runs * args.steps / tp, 'unit': 'run-steps/s',
+                      'how': 'each run through its own CUDA graph, runs one after another'},
+            'plain_concurrent': {'value': args.runs * args.steps / tc, 'unit': 'run-steps/s',
+                                 'how': 'each run through its own CUDA graph on its own stream, all issued at once'},
+            'batched_over_plain': tp / tb,
+            'batched_over_plain_concurrent': tc / tb,
+            'pushes_per_second': nparticles * world * args.steps / tb,
+            'gpu_launches': launches,
+        }))
+    batch.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument('--workload', default='plasma', choices=['plasma', 'ensemble'])
+    ap.add_argument('--runs', type=int, default=256, help='ensemble runs (--workload ensemble)')
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=3)
@@ -352,6 +465,8 @@ def main():
     try:
         if args.impl == 'reference':
             rc = run_reference(args, world, rank)
+        elif args.workload == 'ensemble':
+            rc = run_ensemble(args, world, rank, local)
         else:
             rc = run_gpu(args, world, rank, local)
     finally:

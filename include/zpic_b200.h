@@ -196,6 +196,14 @@ int zpic_b200_species_set( zpic_sim * sim, int32_t sp, const int32_t * np,
 int zpic_b200_species_gather( zpic_sim * sim, int32_t sp, int32_t quant, float * out );
 /* Species::deposit_charge + add_from_gc as save_charge builds it (species.cpp:2486-2511); dense [ny][nx] */
 int zpic_b200_species_charge( zpic_sim * sim, int32_t sp, float * out );
+/* Species::dep_phasespace (species.cpp:2631-2709 1D, 2863-3022 2D): phase-space
+ * density of a species into out[size0] (quant1 < 0) or out[size1][size0].
+ * Quantities: ZPIC_PHA_X, _Y (positions, range in simulation units), _UX, _UY,
+ * _UZ.  A 2D phase space needs quant1 > quant0 (the reference's rule).  The
+ * bins are FP32 sums like the reference's; their order of summation differs. */
+enum { ZPIC_PHA_X = 0, ZPIC_PHA_Y = 1, ZPIC_PHA_UX = 2, ZPIC_PHA_UY = 3, ZPIC_PHA_UZ = 4 };
+int zpic_b200_species_phasespace( zpic_sim * sim, int32_t sp, int32_t quant0, const float range0[2], int32_t size0,
+                                  int32_t quant1, const float range1[2], int32_t size1, float * out );
 
 /* ---- grids (grid.h / vec3grid.h) ---- */
 /* cells in the tiled buffer, guard cells and padding included: ntiles * tile_vol */
@@ -234,6 +242,10 @@ int zpic_b200_batch_create( zpic_sim * const * sims, int32_t n, zpic_batch ** ou
 int zpic_b200_batch_advance( zpic_batch * batch, int32_t nsteps );
 int zpic_b200_batch_synchronize( zpic_batch * batch );
 int zpic_b200_batch_destroy( zpic_batch * batch );
+/* Kernel launches issued by batch steps since the batch was created. */
+int zpic_b200_batch_launch_count( zpic_batch * batch, uint64_t * count );
+/* The cudaStream_t a batch's steps run on (for external event timing). */
+int zpic_b200_batch_stream( zpic_batch * batch, void ** stream );
 
 #ifdef __cplusplus
 }

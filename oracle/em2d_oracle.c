@@ -1750,6 +1750,14 @@ void osim_current_zero( osim * s ) { grid_zero( &s->cur.J ); }
 void osim_current_advance( osim * s ) { current_advance( &s->cur ); }
 void osim_emf_advance( osim * s, int with_current ) { emf_advance( &s->emf, with_current ? &s->cur : NULL ); }
 void osim_species_advance( osim * s, int sp ) { species_advance( s, s->sp[sp] ); }
+/* Species::advance() free streaming (species.cpp:1998-2012): move, walls, sort */
+void osim_species_advance_free( osim * s, int sp ) {
+    ospecies * p = s->sp[sp];
+    species_move( p, &s->cur.J, 0, 0, 0 );
+    species_process_bc( p );
+    tile_sort( p->part, p->tmp, &p->sort, NULL );
+    p->iter++;
+}
 void osim_species_push( osim * s, int sp ) { species_push( s->sp[sp], &s->emf.E, &s->emf.B ); }
 void osim_species_move( osim * s, int sp ) { species_move( s->sp[sp], &s->cur.J, 0, 0, 1 ); }
 void osim_species_process_bc( osim * s, int sp ) { species_process_bc( s->sp[sp] ); }
@@ -1820,6 +1828,71 @@ void osim_grid_set( osim * s, int which, const real * in ) {
 }
 
 /* species.cpp:2486-2511 (deposit + add_from_gc + gather), dense output */
+/*
+ * Species::dep_phasespace, 1D (species.cpp:2631-2709) and 2D (2863-3022),
+ * with dep_pha1_kernel (2579-2620) / dep_pha2_kernel (2786-2852): tiles in
+ * order, particles in order, serial sums.  The normalisation calls fabs() on
+ * the float charge without std::; in the reference build that is C's double
+ * fabs, so the normalisation is evaluated in double and rounded once.
+ * Returns -1 for an invalid 2D pair (quant1 <= quant0).
+ */
+static real pha_value( int q, int shiftx, int shifty, const int * ix, const real * x, const real * u ) {
+    switch ( q ) {
+    case 0:  return ( shiftx + ix[0] ) + ( x[0] + (real) 0.5 );
+    case 1:  return ( shifty + ix[1] ) + ( x[1] + (real) 0.5 );
+    case 2:  return u[0];
+    case 3:  return u[1];
+    default: return u[2];
+    }
+}
+
+int osim_species_phasespace( osim * s, int sp, int q0, const float * range0, int size0,
+                             int q1, const float * range1, int size1, real * out ) {
+    ospecies * p = s->sp[sp];
+    oparts * part = p->part;
+    const int two = q1 >= 0;
+    if ( two && q0 >= q1 ) return -1;
+    real r0x = range0[0], r0y = range0[1], r1x = 0, r1y = 0;
+    if ( two ) { r1x = range1[0]; r1y = range1[1]; }
+    real norm;
+    if ( !two ) norm = fabs( (double) p->q ) * ( p->dx.x * p->dx.y ) * (unsigned) size0 / ( r0y - r0x );
+    else norm = fabs( (double) p->q ) * ( p->dx.x * p->dx.y ) * ( (unsigned) size0 / ( r0y - r0x ) ) *
+                ( (unsigned) size1 / ( r1y - r1x ) );
+    if ( q0 == 0 ) { r0y /= p->dx.x; r0x /= p->dx.x; }
+    if ( q0 == 1 ) { r0y /= p->dx.y; r0x /= p->dx.y; }
+    if ( two && q1 == 1 ) { r1y /= p->dx.y; r1x /= p->dx.y; }
+    const size_t nbins = (size_t) size0 * ( two ? size1 : 1 );
+    for ( size_t i = 0; i < nbins; i++ ) out[i] = 0;
+    const real rdx0 = size0 / ( r0y - r0x ), rdx1 = two ? size1 / ( r1y - r1x ) : 0;
+    for ( unsigned ty = 0; ty < part->nty; ty++ )
+        for ( unsigned tx = 0; tx < part->ntx; tx++ ) {
+            const int tid = ty * part->ntx + tx;
+            const int shiftx = tx * part->nxx, shifty = ty * part->nxy;
+            for ( int i = 0; i < part->np[tid]; i++ ) {
+                const size_t g = (size_t) part->offset[tid] + i;
+                const int * ix = part->ix + 2 * g; const real * x = part->x + 2 * g; const real * u = part->u + 3 * g;
+                const real n0 = ( pha_value( q0, shiftx, shifty, ix, x, u ) - r0x ) * rdx0 - (real) 0.5;
+                const int k0 = (int) ( n0 + 1 ) - 1;
+                const real w0 = n0 - k0;
+                if ( !two ) {
+                    if ( ( k0 >= 0 ) && ( k0 < size0 - 1 ) ) out[k0] += ( 1 - w0 ) * norm;
+                    if ( ( k0 + 1 >= 0 ) && ( k0 + 1 < size0 - 1 ) ) out[k0 + 1] += w0 * norm;
+                } else {
+                    const real n1 = ( pha_value( q1, shiftx, shifty, ix, x, u ) - r1x ) * rdx1 - (real) 0.5;
+                    const int k1 = (int) ( n1 + 1 ) - 1;
+                    const real w1 = n1 - k1;
+                    const int a0 = ( k0 >= 0 ) && ( k0 < size0 - 1 ), b0 = ( k0 + 1 >= 0 ) && ( k0 + 1 < size0 - 1 );
+                    const int a1 = ( k1 >= 0 ) && ( k1 < size1 - 1 ), b1 = ( k1 + 1 >= 0 ) && ( k1 + 1 < size1 - 1 );
+                    if ( a0 && a1 ) out[k1 * size0 + k0]           += ( 1 - w0 ) * ( 1 - w1 ) * norm;
+                    if ( b0 && a1 ) out[k1 * size0 + k0 + 1]       += w0 * ( 1 - w1 ) * norm;
+                    if ( a0 && b1 ) out[( k1 + 1 ) * size0 + k0]   += ( 1 - w0 ) * w1 * norm;
+                    if ( b0 && b1 ) out[( k1 + 1 ) * size0 + k0 + 1] += w0 * w1 * norm;
+                }
+            }
+        }
+    return 0;
+}
+
 void osim_species_charge( osim * s, int sp, real * out ) {
     ospecies * p = s->sp[sp];
     ogrid ch;

@@ -53,6 +53,7 @@ void     osim_current_zero( osim * s );
 void     osim_current_advance( osim * s );
 void     osim_emf_advance( osim * s, int with_current );
 void     osim_species_advance( osim * s, int sp );
+void     osim_species_advance_free( osim * s, int sp );
 void     osim_species_push( osim * s, int sp );
 void     osim_species_move( osim * s, int sp );
 void     osim_species_process_bc( osim * s, int sp );
@@ -70,5 +71,7 @@ uint64_t osim_grid_size( osim * s, int which );
 void     osim_grid_get( osim * s, int which, real * out );
 void     osim_grid_set( osim * s, int which, const real * in );
 void     osim_species_charge( osim * s, int sp, real * out );
+int      osim_species_phasespace( osim * s, int sp, int q0, const float * range0, int size0,
+                                  int q1, const float * range1, int size1, real * out );
 
 #endif

@@ -114,6 +114,7 @@ class _Sim:
             'current_advance': (None, [P]),
             'emf_advance': (None, [P, I]),
             'species_advance': (None, [P, I]),
+            'species_advance_free': (None, [P, I]),
             'species_push': (None, [P, I]),
             'species_move': (None, [P, I]),
             'species_process_bc': (None, [P, I]),
@@ -130,6 +131,7 @@ class _Sim:
             'grid_get': (None, [P, I, RP]),
             'grid_set': (None, [P, I, RP]),
             'species_charge': (None, [P, I, RP]),
+            'species_phasespace': (I, [P, I, I, FP, I, I, FP, I, RP]),
         }
         for k, (r, a) in tab.items():
             self.f[k.replace('sim_', '') if k.startswith('sim_') else k] = self._fn(k, r, a)
@@ -214,6 +216,10 @@ class _Sim:
     def species_advance(self, sp):
         self.f['species_advance'](self.h, sp)
 
+    def species_advance_free(self, sp):
+        """Species::advance(): free streaming, no fields, no current (species.cpp:1998-2012)."""
+        self.f['species_advance_free'](self.h, sp)
+
     def species_push(self, sp):
         self.f['species_push'](self.h, sp)
 
@@ -287,6 +293,31 @@ class _Sim:
     def set_grid(self, which, data):
         data = np.ascontiguousarray(data, self._rt)
         self.f['grid_set'](self.h, self._WHICH[which], data.ctypes.data_as(self._RP))
+
+    def emf_save(self, field, fc):
+        """EMF::save through the reference build (writes EMF/<name>-<iter>.zdf in the cwd)."""
+        f = self.lib.ref_emf_save
+        f.restype, f.argtypes = None, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        f(self.h, {'E': 0, 'B': 1}[field], int(fc))
+
+    def species_save_charge(self, sp):
+        f = self.lib.ref_species_save_charge
+        f.restype, f.argtypes = None, [ctypes.c_void_p, ctypes.c_int]
+        f(self.h, int(sp))
+
+    def phasespace(self, sp, q0, range0, size0, q1=-1, range1=(0.0, 1.0), size1=1):
+        """Species::dep_phasespace: out[size0] or out[size1, size0]; quantities
+        0 x, 1 y, 2 ux, 3 uy, 4 uz."""
+        FP = ctypes.POINTER(ctypes.c_float)
+        r0 = (ctypes.c_float * 2)(*range0)
+        r1 = (ctypes.c_float * 2)(*range1)
+        shape = (size0,) if q1 < 0 else (size1, size0)
+        out = np.zeros(shape, self._rt)
+        rc = self.f['species_phasespace'](self.h, sp, int(q0), ctypes.cast(r0, FP), int(size0), int(q1),
+                                          ctypes.cast(r1, FP), int(size1), out.ctypes.data_as(self._RP))
+        if rc != 0:
+            raise ValueError('invalid phasespace quantities')
+        return out
 
     def charge(self, sp):
         dims = (self.ntiles[1] * self.nx[1], self.ntiles[0] * self.nx[0])

@@ -204,6 +204,9 @@ void ref_species_advance( void * h, int sp ) {
     RefSim * s = static_cast<RefSim *>( h );
     s->species[sp]->advance( s->sim->emf, s->sim->current );
 }
+void ref_species_advance_free( void * h, int sp ) {
+    static_cast<RefSim *>( h )->species[sp]->advance();
+}
 void ref_species_push( void * h, int sp ) {
     RefSim * s = static_cast<RefSim *>( h );
     s->species[sp]->push( s->sim->emf.E, s->sim->emf.B );
@@ -291,6 +294,32 @@ void ref_grid_get( void * h, int which, float * out ) {
 void ref_grid_set( void * h, int which, const float * in ) {
     vec3grid<float3> * g = pick_grid( static_cast<RefSim *>( h ), which );
     std::memcpy( (void *) g->d_buffer, in, g->buffer_size() * sizeof( float3 ) );
+}
+
+/* ZDF diagnostics written by the reference itself (files under the current directory) */
+void ref_emf_save( void * h, int field, int fc ) {
+    static_cast<RefSim *>( h )->sim->emf.save( field ? emf::b : emf::e, (fcomp::cart) fc );
+}
+void ref_current_save( void * h, int fc ) {
+    static_cast<RefSim *>( h )->sim->current.save( (fcomp::cart) fc );
+}
+void ref_species_save_charge( void * h, int sp ) {
+    static_cast<RefSim *>( h )->species[sp]->save_charge();
+}
+
+/* Species::dep_phasespace, 1D or 2D (quant1 < 0 selects 1D) */
+int ref_species_phasespace( void * h, int sp, int q0, const float * range0, int size0,
+                            int q1, const float * range1, int size1, float * out ) {
+    RefSim * s = static_cast<RefSim *>( h );
+    HSpecies * p = s->species[sp];
+    if ( q1 < 0 ) {
+        p->dep_phasespace( out, (phasespace::quant) q0, make_float2( range0[0], range0[1] ), (unsigned) size0 );
+    } else {
+        if ( q0 >= q1 ) return -1;
+        p->dep_phasespace( out, (phasespace::quant) q0, make_float2( range0[0], range0[1] ), (unsigned) size0,
+                           (phasespace::quant) q1, make_float2( range1[0], range1[1] ), (unsigned) size1 );
+    }
+    return 0;
 }
 
 /* Charge density as Species::save_charge builds it (species.cpp:2499-2511), gathered dense */

@@ -16,6 +16,9 @@ outputs of the reference itself, run here on seeded inputs:
 * lwfa_small.npz     -- 256x64 cells moving window, step density, Gaussian
                         laser (a0 2, omega0 10), compensated filter: particle
                         count and energies every 10 steps to 120
+* diagnostics_small.npz -- the Weibel test set-up after 20 steps: charge
+                        density of both species and 1D / 2D phase spaces
+                        (Species::dep_phasespace) for the PHASESPACES list
 """
 import os
 import sys
@@ -51,7 +54,32 @@ def state(sim, tag):
     return out
 
 
+# (quant0, range0, size0, quant1, range1, size1); quant1 < 0 for 1D
+PHASESPACES = [
+    (0, (0.0, 12.8), 64, -1, (0.0, 1.0), 1),
+    (1, (1.0, 11.0), 33, -1, (0.0, 1.0), 1),
+    (2, (-0.5, 0.5), 100, -1, (0.0, 1.0), 1),
+    (4, (-1.0, 1.0), 77, -1, (0.0, 1.0), 1),
+    (0, (0.0, 12.8), 64, 2, (-0.5, 0.5), 50),
+    (2, (-0.5, 0.5), 40, 4, (-1.2, 1.2), 60),
+    (1, (0.0, 12.8), 32, 3, (-0.4, 0.4), 32),
+]
+
+
+def diagnostics():
+    s = weibel(RefSim((8, 8), (16, 16), (12.8, 12.8), 0.07, threads=1), (4, 4))
+    s.advance(20)
+    d = {}
+    for sp in range(2):
+        d['charge%d' % sp] = s.charge(sp)
+        for k, c in enumerate(PHASESPACES):
+            d['pha%d_%d' % (sp, k)] = s.phasespace(sp, *c)
+    np.savez_compressed(os.path.join(HERE, 'diagnostics_small.npz'), **d)
+    s.close()
+
+
 def main():
+    diagnostics()
     geom = ((4, 4), (8, 8), (3.2, 3.2), 0.07)
     s = weibel(RefSim(*geom, threads=1), (2, 2))
     d = state(s, 's0')

@@ -91,6 +91,21 @@ def test_golden_lwfa_small():
     assert np.array_equal(np.array(hist), g['energy'])
 
 
+def test_golden_diagnostics():
+    """Charge density and phase spaces of the oracle against the reference's
+    (Species::deposit_charge, Species::dep_phasespace) after 20 steps."""
+    import sys
+    sys.path.insert(0, GOLD)
+    from make_golden import PHASESPACES
+    g = np.load(os.path.join(GOLD, 'diagnostics_small.npz'))
+    o = weibel(OracleSim((8, 8), (16, 16), (12.8, 12.8), 0.07))
+    o.advance(20)
+    for sp in range(2):
+        assert np.array_equal(o.charge(sp), g['charge%d' % sp])
+        for k, c in enumerate(PHASESPACES):
+            assert np.array_equal(o.phasespace(sp, *c), g['pha%d_%d' % (sp, k)]), (sp, c)
+
+
 # ---- live reference build ----
 @needs_ref
 def test_pin_weibel_live():

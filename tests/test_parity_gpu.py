@@ -1,7 +1,7 @@
 """Parity of the CUDA em2d step against the oracle (plain-C restatement of the
 reference openmp/em2d build), through the library's C-ABI.
 
-Bars (from the reference's arithmetic, see DESIGN.md):
+Bars (from the reference's arithmetic):
 * per-particle push and move, initial states, tile counts and per-tile
   particle multisets: bit-exact;
 * the Yee solver and the current guard-cell sums on identical inputs: bit-exact;
@@ -76,6 +76,22 @@ def test_euler_push_bit_exact():
 
 def test_move_deposit():
     o, g = pair(weibel)
+    for s in (o, g):
+        s.current_zero()
+    for sp in range(2):
+        o.species_move(sp)
+        g.species_move(sp)
+        a, b = o.particles(sp), g.particles(sp)
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]), 'positions differ'
+    m = interior_mask(o)
+    assert rel_err(g.grid('J')[:, m], o.grid('J')[:, m]) <= J_TOL
+
+
+def test_move_deposit_fp64_tile_current():
+    """Option "jacc": the tile current is summed in FP64 and rounded once per
+    cell; positions stay bit-exact and the current within the FP32 bar."""
+    o, g = pair(weibel)
+    g.set_option('jacc', 1)
     for s in (o, g):
         s.current_zero()
     for sp in range(2):
@@ -219,3 +235,38 @@ def test_walls_filters_profiles():
     for sp in range(2):
         assert o.tiles(sp)[0].sum() == g.tiles(sp)[0].sum()
         assert rel_err(g.species_energy(sp), o.species_energy(sp)) <= 1e-3
+
+
+def test_diagnostics_charge_and_phasespace():
+    """Charge density and 1D / 2D phase spaces (Species::deposit_charge,
+    Species::dep_phasespace) after 20 steps.  Against the oracle evaluated on
+    the same particles: FP32 sums in another order, max|d| <= 1e-5 * max|ref|.
+    Against the reference's committed fixtures (its own trajectory, which
+    differs by the current's rounding): max|d| <= 1e-3 * max|ref|."""
+    import os
+    import sys
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+    sys.path.insert(0, gold)
+    from make_golden import PHASESPACES
+    g = np.load(os.path.join(gold, 'diagnostics_small.npz'))
+    s = weibel(zb.Simulation(*WEIBEL))
+    s.advance(20)
+    o = weibel(OracleSim(*WEIBEL))
+    for sp in range(2):
+        o.set_particles(sp, *s.particles(sp))
+
+    def close(got, ref, tol):
+        assert got.shape == ref.shape
+        return np.abs(got.astype(np.float64) - ref).max() <= tol * np.abs(ref).max()
+    for sp in range(2):
+        got = s.charge(sp)
+        assert close(got, o.charge(sp), 1e-5) and close(got, g['charge%d' % sp], 1e-3)
+        for k, c in enumerate(PHASESPACES):
+            got = s.phasespace(sp, *c)
+            assert close(got, o.phasespace(sp, *c), 1e-5), (sp, c)
+            assert close(got, g['pha%d_%d' % (sp, k)], 1e-3), (sp, c)
+    with pytest.raises(zb.ZpicError):
+        s.phasespace(0, 'ux', (-1, 1), 10, 'x', (0, 12.8), 10)     # 2D needs quant1 > quant0
+    # a large phase space goes through global atomics instead of a shared copy
+    big = s.phasespace(0, 'x', (0.0, 12.8), 256, 'uz', (-1.5, 1.5), 256)
+    assert close(big, o.phasespace(0, 0, (0.0, 12.8), 256, 4, (-1.5, 1.5), 256), 1e-5)

@@ -26,14 +26,17 @@ struct TileItem { int run; int tile; };
 struct InjRule {
     int type; int diry; float a, b; float cx, cy, r2; float dxx, dxy; int ppcx, ppcy; int range[4]; int tx_limit;
 };
-size_t particle_smem_bytes( int tile_vol );
-cudaError_t launch_particles( cudaStream_t, int, int, int, const Item *, int, const SpDev *, const RunDev *, const int *, int );
+size_t particle_smem_bytes( int tile_vol, int jacc );
+size_t yee_smem_bytes( int tile_vol );
+cudaError_t launch_particles( cudaStream_t, int, int, int, const Item *, int, const SpDev *, const RunDev *, const int *,
+                              int, int );
 cudaError_t launch_sort( cudaStream_t, const Item *, int, const SpDev *, const int *, int, const RunDev *, int );
 cudaError_t launch_inject( cudaStream_t, int, int, const SpDev *, const RunDev *, const InjRule &, int );
 cudaError_t launch_pack( cudaStream_t, int, int, const SpDev *, const int *, int2 *, float2 *, float * );
 cudaError_t launch_unpack( cudaStream_t, int, int, const SpDev *, const int *, const int2 *, const float2 *, const float * );
 cudaError_t launch_gather( cudaStream_t, int, int, const SpDev *, const RunDev *, const int *, int, float, float, int, float * );
 cudaError_t launch_dep_charge( cudaStream_t, int, int, const SpDev *, const RunDev *, float *, int, int );
+cudaError_t launch_phasespace( cudaStream_t, int, int, const SpDev *, const RunDev *, PhaSpec, float * );
 cudaError_t launch_energy_sum( cudaStream_t, const SpDev *, int, int, double * );
 cudaError_t launch_np_stats( cudaStream_t, const SpDev *, int, unsigned long long * );
 cudaError_t launch_current_gc( cudaStream_t, const TileItem *, int, const RunDev * );
@@ -117,6 +120,7 @@ struct HSpecies {
     SpDev d{};                // descriptor (device pointers)
     bool sort_pending = false;
     bool counters_dirty = false;
+    int energy_items = 0;      // per-item energy partials written by the last push
 
     void free_all() {
         PartArrays * arrs[3] = { &d.A, &d.B, &d.S };
@@ -148,8 +152,12 @@ struct Plan {
     Item * k1_items_d[2] = { nullptr, nullptr }; int n_k1[2] = { 0, 0 };   // boris, euler
     Item * sort_items_d = nullptr; int n_sort = 0;
     int * splist_d = nullptr; int n_sp = 0;
+    // the same work lists grouped per species (fine-grained species calls)
+    Item * spk1_d = nullptr;
+    std::vector<int> sp_k1_off, sp_k1_n, sp_sort_off, sp_sort_n;
     TileItem * tile_items_d = nullptr; int n_tiles = 0;
     int max_tile_vol = 0;
+    int jacc = 0;                   // FP64 tile current accumulation
     bool needs_bc_or_filter = false;
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
@@ -158,7 +166,7 @@ struct Plan {
     void release() {
         if ( graph ) { cudaGraphExecDestroy( graph ); graph = nullptr; }
         dfree( runs_d ); dfree( sps_d ); dfree( k1_items_d[0] ); dfree( k1_items_d[1] );
-        dfree( sort_items_d ); dfree( splist_d ); dfree( tile_items_d );
+        dfree( sort_items_d ); dfree( splist_d ); dfree( tile_items_d ); dfree( spk1_d );
         built = false;
     }
 };
@@ -193,6 +201,7 @@ struct zpic_sim {
     // options
     bool use_graph = true;
     int chunks_opt = 0;
+    int jacc = 0;
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[PH_N];
     double phase_ms[PH_N] = { 0 };
@@ -208,6 +217,7 @@ struct zpic_batch {
     cudaStream_t stream = nullptr;
     Plan plan;
     cudaEvent_t ev = nullptr;
+    uint64_t launches = 0;          // kernels launched by batch steps
 };
 
 static int sim_select( zpic_sim * s ) {
@@ -256,18 +266,24 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims ) {
     P.release();
     P.sims = sims;
     std::vector<RunDev> runs;
-    std::vector<Item> k1[2], sort_items;
+    std::vector<Item> k1[2], sort_items, spk1;
     std::vector<int> splist;
     std::vector<TileItem> tiles;
     P.sps_h.clear(); P.sp_sim.clear(); P.sp_local.clear();
+    P.sp_k1_off.clear(); P.sp_k1_n.clear(); P.sp_sort_off.clear(); P.sp_sort_n.clear();
     P.max_tile_vol = 0;
+    P.jacc = 0;
     P.needs_bc_or_filter = false;
     int total_tiles = 0;
     for ( auto * s : sims ) for ( auto * sp : s->species ) { (void) sp; total_tiles += s->ntx * s->nty; }
+    // a batch chooses its CTAs per tile from all of its tiles; a single
+    // simulation keeps the choice made for it
+    const int batch_chunks = sims.size() > 1 ? auto_chunks( std::max( 1, total_tiles ), 0 ) : 0;
     for ( size_t r = 0; r < sims.size(); r++ ) {
         zpic_sim * s = sims[r];
         runs.push_back( s->run );
         P.max_tile_vol = std::max( P.max_tile_vol, s->run.tile_vol );
+        P.jacc = std::max( P.jacc, s->jacc );
         for ( int t = 0; t < s->ntx * s->nty; t++ ) tiles.push_back( { (int) r, t } );
         for ( int k = 0; k < 4; k++ )
             if ( s->emf_bc[k] > ZPIC_EMF_BC_PERIODIC || s->cur_bc[k] > ZPIC_CURRENT_BC_PERIODIC ) P.needs_bc_or_filter = true;
@@ -278,15 +294,23 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims ) {
         for ( size_t k = 0; k < s->species.size(); k++ ) {
             HSpecies * sp = s->species[k];
             SpDev d = sp->d;
+            if ( batch_chunks ) d.nchunk = batch_chunks;
             d.run = (int) r;
             const int gi = (int) P.sps_h.size();
             P.sps_h.push_back( d );
             P.sp_sim.push_back( (int) r ); P.sp_local.push_back( (int) k );
             splist.push_back( gi );
+            P.sp_k1_off.push_back( (int) spk1.size() );
+            P.sp_sort_off.push_back( (int) sort_items.size() );
             for ( int t = 0; t < sp->ntiles; t++ ) {
-                for ( int c = 0; c < d.nchunk; c++ ) k1[ sp->push_type ? 1 : 0 ].push_back( { gi, t, c, 0 } );
+                for ( int c = 0; c < d.nchunk; c++ ) {
+                    k1[ sp->push_type ? 1 : 0 ].push_back( { gi, t, c, 0 } );
+                    spk1.push_back( { gi, t, c, 0 } );
+                }
                 sort_items.push_back( { gi, t, 0, 0 } );
             }
+            P.sp_k1_n.push_back( (int) spk1.size() - P.sp_k1_off.back() );
+            P.sp_sort_n.push_back( (int) sort_items.size() - P.sp_sort_off.back() );
         }
     }
     P.n_sp = (int) splist.size();
@@ -308,6 +332,9 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims ) {
         if ( !k1[p].empty() )
             CK( cudaMemcpy( P.k1_items_d[p], k1[p].data(), k1[p].size() * sizeof( Item ), cudaMemcpyHostToDevice ) );
     }
+    TRY( dalloc( &P.spk1_d, spk1.size() ) );
+    if ( !spk1.empty() )
+        CK( cudaMemcpy( P.spk1_d, spk1.data(), spk1.size() * sizeof( Item ), cudaMemcpyHostToDevice ) );
     P.n_sort = (int) sort_items.size();
     P.n_tiles = (int) tiles.size();
     P.built = true;
@@ -353,7 +380,8 @@ static int run_particles( Plan & P, cudaStream_t st, int push, int move, const i
     for ( int p = 0; p < 2; p++ ) {
         if ( P.n_k1[p] == 0 ) continue;
         PhaseScope ps( prof_sim( P ), st, PH_PARTICLES, 1 );
-        CK( launch_particles( st, push ? p + 1 : 0, move, 1, P.k1_items_d[p], P.n_k1[p], P.sps_d, P.runs_d, shifts, P.max_tile_vol ) );
+        CK( launch_particles( st, push ? p + 1 : 0, move, 1, P.k1_items_d[p], P.n_k1[p], P.sps_d, P.runs_d, shifts, P.max_tile_vol,
+                              P.jacc ) );
     }
     return ZPIC_OK;
 }
@@ -466,6 +494,8 @@ static int plan_step_device( Plan & P, cudaStream_t st ) {
 }
 
 static void plan_step_host( Plan & P ) {
+    for ( size_t g = 0; g < P.sps_h.size(); g++ )
+        P.sims[ P.sp_sim[g] ]->species[ P.sp_local[g] ]->energy_items = P.sps_h[g].ntiles * P.sps_h[g].nchunk;
     for ( auto * s : P.sims ) {
         for ( auto * sp : s->species ) { sp->iter++; sp->sort_pending = false; sp->counters_dirty = false; }
         s->cur_iter++;
@@ -653,10 +683,8 @@ static int species_index( zpic_sim * s, int sp ) {
     return ZPIC_OK;
 }
 
-// plan-level species index of local species sp in a single-sim plan
-static int plan_sp( zpic_sim * s, int sp ) { (void) s; return sp; }
-
-// Launch the particle kernel for one species of a single simulation.
+// Launch the particle kernel for one species of a single simulation (no host
+// synchronisation; errors surface at the next synchronising call).
 static int species_kernel( zpic_sim * s, int sp, int push, int move, const int * shifts ) {
     TRY( ensure_plan( s ) );
     HSpecies * h = s->species[sp];
@@ -664,20 +692,15 @@ static int species_kernel( zpic_sim * s, int sp, int push, int move, const int *
         CK( cudaMemsetAsync( h->d.npt, 0, 9 * h->ntiles * sizeof( int ), s->stream ) );
         CK( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
     }
-    // items of this species: rebuild a small list (per-species launches are the fine-grained API path)
-    std::vector<Item> items;
-    for ( int t = 0; t < h->ntiles; t++ ) for ( int c = 0; c < h->d.nchunk; c++ ) items.push_back( { plan_sp( s, sp ), t, c, 0 } );
-    Item * items_d = nullptr;
-    TRY( dalloc( &items_d, items.size() ) );
-    CK( cudaMemcpyAsync( items_d, items.data(), items.size() * sizeof( Item ), cudaMemcpyHostToDevice, s->stream ) );
+    Plan & P = s->plan;
     {
         PhaseScope ps( s, s->stream, PH_PARTICLES, 1 );
-        CK( launch_particles( s->stream, push ? 1 + h->push_type : 0, move, move ? 1 : 0, items_d, (int) items.size(),
-                              s->plan.sps_d, s->plan.runs_d, shifts, s->plan.max_tile_vol ) );
+        CK( launch_particles( s->stream, push ? 1 + h->push_type : 0, move, move ? 1 : 0,
+                              P.spk1_d + P.sp_k1_off[sp], P.sp_k1_n[sp], P.sps_d, P.runs_d, shifts, P.max_tile_vol,
+                              P.jacc ) );
     }
-    CK( cudaStreamSynchronize( s->stream ) );
-    dfree( items_d );
     if ( move ) { h->sort_pending = true; h->counters_dirty = true; }
+    if ( push ) h->energy_items = h->ntiles * P.sps_h[sp].nchunk;
     if ( move == 2 ) s->jdep_clean = false;
     return ZPIC_OK;
 }
@@ -685,37 +708,23 @@ static int species_kernel( zpic_sim * s, int sp, int push, int move, const int *
 static int species_sort( zpic_sim * s, int sp, int use_extra ) {
     TRY( ensure_plan( s ) );
     HSpecies * h = s->species[sp];
+    Plan & P = s->plan;
     if ( !h->sort_pending ) {
         // leaver lists are stale: detect them now (bnd_check, particles.cpp:212-303)
         CK( cudaMemsetAsync( h->d.npt, 0, 9 * h->ntiles * sizeof( int ), s->stream ) );
         CK( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
-        std::vector<Item> items;
-        for ( int t = 0; t < h->ntiles; t++ ) items.push_back( { sp, t, 0, 0 } );
-        Item * items_d = nullptr;
-        TRY( dalloc( &items_d, items.size() ) );
-        CK( cudaMemcpyAsync( items_d, items.data(), items.size() * sizeof( Item ), cudaMemcpyHostToDevice, s->stream ) );
-        {
-            PhaseScope ps( s, s->stream, PH_SORT, 1 );
-            CK( launch_particles( s->stream, 0, 0, 1, items_d, (int) items.size(), s->plan.sps_d, s->plan.runs_d, nullptr, s->plan.max_tile_vol ) );
-        }
-        CK( cudaStreamSynchronize( s->stream ) );
-        dfree( items_d );
+        PhaseScope ps( s, s->stream, PH_SORT, 1 );
+        CK( launch_particles( s->stream, 0, 0, 1, P.spk1_d + P.sp_k1_off[sp], P.sp_k1_n[sp], P.sps_d, P.runs_d,
+                              nullptr, P.max_tile_vol, 0 ) );
     }
-    std::vector<Item> items;
-    for ( int t = 0; t < h->ntiles; t++ ) items.push_back( { sp, t, 0, 0 } );
-    Item * items_d = nullptr; int * list_d = nullptr;
-    TRY( dalloc( &items_d, items.size() ) ); TRY( dalloc( &list_d, 1 ) );
-    CK( cudaMemcpyAsync( items_d, items.data(), items.size() * sizeof( Item ), cudaMemcpyHostToDevice, s->stream ) );
-    CK( cudaMemcpyAsync( list_d, &sp, sizeof( int ), cudaMemcpyHostToDevice, s->stream ) );
     {
         PhaseScope ps( s, s->stream, PH_SORT, 3 );
-        CK( launch_sort( s->stream, items_d, (int) items.size(), s->plan.sps_d, list_d, 1, s->plan.runs_d, use_extra ) );
+        CK( launch_sort( s->stream, P.sort_items_d + P.sp_sort_off[sp], P.sp_sort_n[sp], P.sps_d,
+                         P.splist_d + sp, 1, P.runs_d, use_extra ) );
     }
-    CK( cudaStreamSynchronize( s->stream ) );
-    dfree( items_d ); dfree( list_d );
     h->sort_pending = false;
     h->counters_dirty = false;
-    return check_status( s );
+    return ZPIC_OK;
 }
 
 // Species::advance_mov_window (species.cpp:2083-2128) for one species
@@ -785,7 +794,13 @@ int zpic_b200_sim_create( uint32_t ntx, uint32_t nty, uint32_t nxx, uint32_t nxy
     *out = nullptr;
     if ( ntx == 0 || nty == 0 ) return fail( ZPIC_E_INVALID, "Invalid number of tiles" );      // grid.h:34-38
     if ( nxx == 0 || nxy == 0 ) return fail( ZPIC_E_INVALID, "Invalid tile size" );            // grid.h:40-43
-    if ( nxx > 4096 || nxy > 4096 ) return fail( ZPIC_E_INVALID, "tile size above 4096 cells" );
+    {
+        // every tile kernel stages whole tiles in shared memory (227 KB per block)
+        const int tv = roundup4( ( nxx + 3 ) * ( nxy + 3 ) );
+        const size_t need = std::max( particle_smem_bytes( tv, 1 ), yee_smem_bytes( tv ) );
+        if ( nxx > 1024 || nxy > 1024 || need > 227 * 1024 )
+            return fail( ZPIC_E_INVALID, "tile too large: its field tiles do not fit in shared memory" );
+    }
     // Courant condition (emf.cpp:20-28)
     const float dxx = boxx / ( nxx * ntx ), dxy = boxy / ( nxy * nty );
     const float cour = std::sqrt( 1.0f / ( 1.0f / ( dxx * dxx ) + 1.0f / ( dxy * dxy ) ) );
@@ -936,18 +951,16 @@ int zpic_b200_sim_set_option( zpic_sim * s, const char * key, double v ) {
     std::string k( key );
     if ( k == "graph" ) { s->use_graph = v != 0; }
     else if ( k == "profile" ) { s->profile = v != 0; if ( s->profile ) s->use_graph = false; }
+    else if ( k == "jacc" ) {
+        const int j = v != 0 ? 1 : 0;
+        if ( j != s->jacc ) { s->jacc = j; s->plan.release(); }
+    }
     else if ( k == "chunks" ) {
-        s->chunks_opt = (int) v;
+        // the per-item energy array holds 64 chunks per tile
+        s->chunks_opt = std::min( 64, std::max( 0, (int) v ) );
         int ntot = 0; for ( auto * h : s->species ) ntot += h->ntiles;
         const int ch = auto_chunks( std::max( 1, ntot ), s->chunks_opt );
-        for ( auto * h : s->species ) {
-            if ( h->d.nchunk != ch ) {
-                dfree( h->d.energy );
-                TRY( dalloc( &h->d.energy, (size_t) h->ntiles * ch ) );
-                CK( cudaMemset( h->d.energy, 0, (size_t) h->ntiles * ch * sizeof( double ) ) );
-                h->d.nchunk = ch;
-            }
-        }
+        for ( auto * h : s->species ) h->d.nchunk = ch;
         s->plan.release();
     }
     else return fail( ZPIC_E_INVALID, "unknown option " + k );
@@ -1190,15 +1203,19 @@ int zpic_b200_species_set_bc( zpic_sim * s, int32_t sp, const int32_t bc[4] ) {
 
 int zpic_b200_species_set_push_type( zpic_sim * s, int32_t sp, int32_t type ) {
     TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
-    s->species[sp]->push_type = type ? 1 : 0;
-    s->plan.release();
+    const int t = type ? 1 : 0;
+    if ( s->species[sp]->push_type != t ) {
+        s->species[sp]->push_type = t;
+        s->plan.release();
+    }
     return ZPIC_OK;
 }
 
 int zpic_b200_species_energy( zpic_sim * s, int32_t sp, double * energy ) {
     TRY( sim_select( s ) ); TRY( species_index( s, sp ) ); TRY( ensure_plan( s ) );
     HSpecies * h = s->species[sp];
-    CK( launch_energy_sum( s->stream, s->plan.sps_d, sp, h->ntiles * h->d.nchunk, s->dscratch ) );
+    const int items = h->energy_items > 0 ? h->energy_items : h->ntiles * h->d.nchunk;
+    CK( launch_energy_sum( s->stream, s->plan.sps_d, sp, items, s->dscratch ) );
     s->launches++;
     double d = 0;
     CK( cudaMemcpyAsync( &d, s->dscratch, sizeof( double ), cudaMemcpyDeviceToHost, s->stream ) );
@@ -1321,6 +1338,7 @@ int zpic_b200_species_gather( zpic_sim * s, int32_t sp, int32_t quant, float * o
 int zpic_b200_species_charge( zpic_sim * s, int32_t sp, float * out ) {
     TRY( sim_select( s ) ); TRY( species_index( s, sp ) ); TRY( ensure_plan( s ) );
     HSpecies * h = s->species[sp];
+    if ( h->sort_pending ) return fail( ZPIC_E_INVALID, "particles have moved since the last tile sort" );
     const int cextx = s->nxx + 1, cexty = s->nxy + 1;
     const int cvol = roundup4( cextx * cexty );
     const size_t nraw = (size_t) cvol * h->ntiles;
@@ -1336,6 +1354,56 @@ int zpic_b200_species_charge( zpic_sim * s, int32_t sp, float * out ) {
     CK( cudaStreamSynchronize( s->stream ) );
     dfree( raw ); dfree( dense );
     return ZPIC_OK;
+}
+
+// Species::dep_phasespace, 1D (species.cpp:2631-2709) and 2D (2863-3022).
+// The reference's normalisation calls C's double fabs() on the float charge,
+// so that expression is evaluated in double and rounded once to float; the
+// range scaling is FP32.
+int zpic_b200_species_phasespace( zpic_sim * s, int32_t sp, int32_t quant0, const float range0[2], int32_t size0,
+                                  int32_t quant1, const float range1[2], int32_t size1, float * out ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) ); TRY( ensure_plan( s ) );
+    if ( !range0 || !out || quant0 < 0 || quant0 > 4 || size0 <= 0 )
+        return fail( ZPIC_E_INVALID, "invalid phasespace quantity, range or size" );
+    const bool two = quant1 >= 0;
+    if ( two ) {
+        if ( !range1 || quant1 > 4 || size1 <= 0 ) return fail( ZPIC_E_INVALID, "invalid phasespace quantity, range or size" );
+        if ( quant0 >= quant1 )
+            return fail( ZPIC_E_INVALID, "for 2D phasespaces, the 2nd quantity must be indexed higher than the first one" );
+    }
+    HSpecies * h = s->species[sp];
+    if ( h->sort_pending ) return fail( ZPIC_E_INVALID, "particles have moved since the last tile sort" );
+    float r0[2] = { range0[0], range0[1] }, r1[2] = { 0, 0 };
+    if ( two ) { r1[0] = range1[0]; r1[1] = range1[1]; }
+    if ( !( r0[1] != r0[0] ) || ( two && !( r1[1] != r1[0] ) ) ) return fail( ZPIC_E_INVALID, "empty phasespace range" );
+    PhaSpec p{};
+    p.q0 = quant0; p.q1 = two ? quant1 : -1; p.n0 = size0; p.n1 = two ? size1 : 1;
+    const float dxy = h->dx[0] * h->dx[1];
+    const double aq = std::fabs( (double) h->q );
+    if ( !two ) {
+        const unsigned usize = (unsigned) size0;
+        p.norm = (float) ( aq * dxy * usize / ( r0[1] - r0[0] ) );
+    } else {
+        const unsigned u0 = (unsigned) size0, u1 = (unsigned) size1;
+        p.norm = (float) ( aq * dxy * ( u0 / ( r0[1] - r0[0] ) ) * ( u1 / ( r1[1] - r1[0] ) ) );
+    }
+    // positions are deposited in cell units
+    for ( int k = 0; k < 2; k++ ) {
+        if ( quant0 < 2 ) r0[k] /= h->dx[ quant0 ];
+        if ( two && quant1 < 2 ) r1[k] /= h->dx[ quant1 ];
+    }
+    p.r0 = r0[0]; p.rdx0 = size0 / ( r0[1] - r0[0] );
+    if ( two ) { p.r1 = r1[0]; p.rdx1 = size1 / ( r1[1] - r1[0] ); }
+    const size_t nbins = (size_t) size0 * ( two ? size1 : 1 );
+    float * d = nullptr;
+    TRY( dalloc( &d, nbins ) );
+    CK( cudaMemsetAsync( d, 0, nbins * sizeof( float ), s->stream ) );
+    CK( launch_phasespace( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, p, d ) );
+    s->launches += 1;
+    CK( cudaMemcpyAsync( out, d, nbins * sizeof( float ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    dfree( d );
+    return check_status( s );
 }
 
 // ---- grids ----
@@ -1423,11 +1491,21 @@ int zpic_b200_batch_advance( zpic_batch * b, int32_t nsteps ) {
     }
     uint64_t l = 0;
     TRY( plan_advance( b->plan, b->stream, nsteps, true, &l ) );
+    b->launches += l;
     CK( cudaEventRecord( b->ev, b->stream ) );
-    for ( auto * s : b->sims ) {
-        CK( cudaStreamWaitEvent( s->stream, b->ev, 0 ) );
-        s->launches += l / b->sims.size();
-    }
+    for ( auto * s : b->sims ) CK( cudaStreamWaitEvent( s->stream, b->ev, 0 ) );
+    return ZPIC_OK;
+}
+
+int zpic_b200_batch_launch_count( zpic_batch * b, uint64_t * count ) {
+    if ( !b || !count ) return fail( ZPIC_E_INVALID, "null argument" );
+    *count = b->launches;
+    return ZPIC_OK;
+}
+
+int zpic_b200_batch_stream( zpic_batch * b, void ** stream ) {
+    if ( !b || !stream ) return fail( ZPIC_E_INVALID, "null argument" );
+    *stream = (void *) b->stream;
     return ZPIC_OK;
 }
 

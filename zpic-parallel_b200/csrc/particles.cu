@@ -7,6 +7,8 @@
 // push and move are therefore bit-identical to the reference.
 #include "zpic_dev.cuh"
 
+#include <algorithm>
+
 namespace zb {
 
 // ---------------------------------------------------------------------------
@@ -234,7 +236,10 @@ __device__ __forceinline__ void drain_entry( const CrossQueue & Q, int e, float 
 constexpr int PK_THREADS = 256;
 constexpr int PK_PPT = 2;                   // particles per thread per block iteration
 
-template < int PUSH, int MOVE, bool DETECT >
+// JT is the type of the tile current accumulated in shared memory: float
+// (the reference's FP32 sums) or double (FP64 accumulation, rounded to FP32
+// once per cell when the tile is added to the global deposit buffer).
+template < int PUSH, int MOVE, bool DETECT, typename JT = float >
 __global__ void __launch_bounds__( PK_THREADS, 4 )
 k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
              const RunDev * __restrict__ runs, const int * __restrict__ shifts )
@@ -247,9 +252,11 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     const int t = it.tile;
     const int nchunk = S.nchunk;
 
+    // shared memory: [E tile][B tile][tile current (JT)][mbarrier]
+    //                [energy partials][crossing queues]
     float * sE = reinterpret_cast<float *>( smem_raw );
     float * sB = sE + 3 * tv;
-    float * sJ = sB + 3 * tv;
+    JT * sJ = reinterpret_cast<JT *>( sB + 3 * tv );
     uint64_t * bar = reinterpret_cast<uint64_t *>( sJ + 3 * tv );
     double * sred = reinterpret_cast<double *>( bar + 1 );
     CrossQueue * xq = reinterpret_cast<CrossQueue *>( sred + PK_THREADS / 32 );
@@ -280,7 +287,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
         }
     }
     if ( MOVE == 2 ) {
-        for ( int i = threadIdx.x; i < 3 * tv; i += blockDim.x ) sJ[i] = 0.0f;
+        for ( int i = threadIdx.x; i < 3 * tv; i += blockDim.x ) sJ[i] = (JT) 0;
     }
     if ( PUSH ) mbar_wait_bounded( bar, 0, R.status );
     __syncthreads();
@@ -288,7 +295,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     const int ys = R.extx;
     const float * Ec = sE + 3 * R.gc_off;
     const float * Bc = sB + 3 * R.gc_off;
-    float * Jc = sJ + 3 * R.gc_off;
+    JT * Jc = sJ + 3 * R.gc_off;
     const int nxx = R.nxx, nxy = R.nxy;
     const int tx = t % R.ntx, ty = t / R.ntx;
     const int shift = ( MOVE && shifts ) ? shifts[ it.sp ] : 0;
@@ -454,6 +461,13 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
         if ( lane == 0 ) sred[ threadIdx.x >> 5 ] = energy;
     }
     __syncthreads();
+    const float * sJout = reinterpret_cast<const float *>( sJ );
+    if ( MOVE == 2 && sizeof( JT ) == 8 ) {
+        // round the FP64 tile current once per cell, into the E tile's place
+        for ( int i = threadIdx.x; i < 3 * tv; i += blockDim.x ) sE[i] = (float) sJ[i];
+        sJout = sE;
+        __syncthreads();
+    }
     if ( threadIdx.x == 0 ) {
         if ( PUSH ) {
             double e = 0.0;
@@ -463,7 +477,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
         if ( MOVE && it.chunk == 0 ) atomicAdd( S.nmove, (unsigned long long) np );
         if ( MOVE == 2 ) {
             fence_proxy_async_smem();
-            bulk_s2g_add_f32( R.Jdep + (size_t) t * 3 * tv, sJ, 12u * tv );
+            bulk_s2g_add_f32( R.Jdep + (size_t) t * 3 * tv, sJout, 12u * tv );
             bulk_commit();
             bulk_wait_all();
         }
@@ -900,6 +914,71 @@ __global__ void k_dep_charge( int sp, const SpDev * __restrict__ sps, const RunD
     (void) runs;
 }
 
+// Phase-space density of one species (dep_pha1_kernel species.cpp:2579-2620,
+// dep_pha2_kernel 2786-2852): every particle adds linear weights to two (1D)
+// or four (2D) bins; bins k with k < 0 or k >= size-1 receive nothing (the
+// reference's bound, which leaves the last bin empty).  Quantities:
+// 0 x, 1 y (cell units, tile shift included), 2 ux, 3 uy, 4 uz.  With
+// PhaSpec::smem the CTA accumulates into a shared-memory copy of the whole
+// phase space and adds its non-zero bins to the output at the end.
+__device__ __forceinline__ float pha_quant( int q, int shiftx, int shifty, uint32_t c,
+                                            float xx, float xy, float ux, float uy, float uz ) {
+    switch ( q ) {
+    case 0:  return (float) ( shiftx + cell_x( c ) ) + ( xx + 0.5f );
+    case 1:  return (float) ( shifty + cell_y( c ) ) + ( xy + 0.5f );
+    case 2:  return ux;
+    case 3:  return uy;
+    default: return uz;
+    }
+}
+
+__global__ void k_phasespace( int sp, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs,
+                              PhaSpec p, float * __restrict__ out )
+{
+    extern __shared__ float sh[];
+    const SpDev & S = sps[sp];
+    const RunDev & R = runs[ S.run ];
+    const bool two = p.q1 >= 0;
+    const int nbins = p.n0 * ( two ? p.n1 : 1 );
+    float * h = p.smem ? sh : out;
+    if ( p.smem ) {
+        for ( int i = threadIdx.x; i < nbins; i += blockDim.x ) sh[i] = 0.f;
+        __syncthreads();
+    }
+    const int ntiles = R.ntx * R.nty;
+    for ( int t = blockIdx.x; t < ntiles; t += gridDim.x ) {
+        const int np = S.np[t], off = S.off[t];
+        const int shiftx = ( t % R.ntx ) * R.nxx, shifty = ( t / R.ntx ) * R.nxy;
+        for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
+            const size_t g = (size_t) off + i;
+            const uint32_t c = S.A.cell[g];
+            const float xx = S.A.xx[g], xy = S.A.xy[g], ux = S.A.ux[g], uy = S.A.uy[g], uz = S.A.uz[g];
+            const float n0 = ( pha_quant( p.q0, shiftx, shifty, c, xx, xy, ux, uy, uz ) - p.r0 ) * p.rdx0 - 0.5f;
+            const int k0 = int( n0 + 1 ) - 1;
+            const float w0 = n0 - k0;
+            const bool a0 = k0 >= 0 && k0 < p.n0 - 1, b0 = k0 + 1 >= 0 && k0 + 1 < p.n0 - 1;
+            if ( !two ) {
+                if ( a0 ) atomicAdd( h + k0, ( 1 - w0 ) * p.norm );
+                if ( b0 ) atomicAdd( h + k0 + 1, w0 * p.norm );
+            } else {
+                const float n1 = ( pha_quant( p.q1, shiftx, shifty, c, xx, xy, ux, uy, uz ) - p.r1 ) * p.rdx1 - 0.5f;
+                const int k1 = int( n1 + 1 ) - 1;
+                const float w1 = n1 - k1;
+                const bool a1 = k1 >= 0 && k1 < p.n1 - 1, b1 = k1 + 1 >= 0 && k1 + 1 < p.n1 - 1;
+                if ( a0 && a1 ) atomicAdd( h + k1 * p.n0 + k0,           ( 1 - w0 ) * ( 1 - w1 ) * p.norm );
+                if ( b0 && a1 ) atomicAdd( h + k1 * p.n0 + k0 + 1,       w0 * ( 1 - w1 ) * p.norm );
+                if ( a0 && b1 ) atomicAdd( h + ( k1 + 1 ) * p.n0 + k0,   ( 1 - w0 ) * w1 * p.norm );
+                if ( b0 && b1 ) atomicAdd( h + ( k1 + 1 ) * p.n0 + k0 + 1, w0 * w1 * p.norm );
+            }
+        }
+    }
+    if ( p.smem ) {
+        __syncthreads();
+        for ( int i = threadIdx.x; i < nbins; i += blockDim.x )
+            if ( sh[i] != 0.f ) atomicAdd( out + i, sh[i] );
+    }
+}
+
 // Per-item energy sums reduced per species in item order (deterministic).
 __global__ void k_energy_sum( const SpDev * __restrict__ sps, int sp, int nitems, double * __restrict__ out )
 {
@@ -942,14 +1021,20 @@ __global__ void k_np_stats( const SpDev * __restrict__ sps, int sp, unsigned lon
 // ---------------------------------------------------------------------------
 namespace zb {
 
-size_t particle_smem_bytes( int tile_vol ) {
-    return (size_t) 3 * 3 * tile_vol * sizeof( float ) + 8 + ( PK_THREADS / 32 ) * sizeof( double ) +
+size_t particle_smem_bytes( int tile_vol, int jacc ) {
+    return (size_t) ( jacc ? 12 : 9 ) * tile_vol * sizeof( float ) + 8 + ( PK_THREADS / 32 ) * sizeof( double ) +
            ( PK_THREADS / 32 ) * sizeof( CrossQueue );
 }
 
 typedef void ( *pk_fn )( const Item *, const SpDev *, const RunDev *, const int * );
 
-static pk_fn pick_particle_kernel( int push, int move, int detect ) {
+static pk_fn pick_particle_kernel( int push, int move, int detect, int jacc ) {
+    if ( jacc && move == 2 ) {
+#define PKD( P, M, D ) if ( push == P && move == M && detect == D ) return k_particles< P, M, D, double >;
+        PKD( 1, 2, true ) PKD( 2, 2, true ) PKD( 0, 2, true )
+#undef PKD
+        return nullptr;
+    }
 #define PK( P, M, D ) if ( push == P && move == M && detect == D ) return k_particles< P, M, D >;
     PK( 1, 2, true ) PK( 2, 2, true )
     PK( 1, 0, false ) PK( 2, 0, false )
@@ -960,10 +1045,12 @@ static pk_fn pick_particle_kernel( int push, int move, int detect ) {
 }
 
 cudaError_t launch_particles( cudaStream_t st, int push, int move, int detect, const Item * items, int nitems,
-                              const SpDev * sps, const RunDev * runs, const int * shifts, int max_tile_vol ) {
-    pk_fn f = pick_particle_kernel( push, move, detect );
+                              const SpDev * sps, const RunDev * runs, const int * shifts, int max_tile_vol,
+                              int jacc ) {
+    jacc = ( jacc && move == 2 ) ? 1 : 0;
+    pk_fn f = pick_particle_kernel( push, move, detect, jacc );
     if ( !f ) return cudaErrorInvalidValue;
-    const size_t smem = particle_smem_bytes( max_tile_vol );
+    const size_t smem = particle_smem_bytes( max_tile_vol, jacc );
     if ( smem > 48 * 1024 )
         cudaFuncSetAttribute( (const void *) f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
     if ( nitems <= 0 ) return cudaSuccess;
@@ -1007,6 +1094,19 @@ cudaError_t launch_gather( cudaStream_t st, int sp, int ntiles, const SpDev * sp
 cudaError_t launch_dep_charge( cudaStream_t st, int sp, int ntiles, const SpDev * sps, const RunDev * runs,
                                float * charge, int cextx, int cvol ) {
     k_dep_charge<<< ntiles, 256, cvol * sizeof( float ), st >>>( sp, sps, runs, charge, cextx, cvol );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_phasespace( cudaStream_t st, int sp, int ntiles, const SpDev * sps, const RunDev * runs,
+                              PhaSpec p, float * out ) {
+    const int nbins = p.n0 * ( p.q1 >= 0 ? p.n1 : 1 );
+    const size_t smem = (size_t) nbins * sizeof( float );
+    // a private copy per CTA when the phase space fits in shared memory
+    p.smem = smem <= 200 * 1024;
+    if ( p.smem && smem > 48 * 1024 )
+        cudaFuncSetAttribute( (const void *) k_phasespace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
+    const int grid = p.smem ? std::min( ntiles, 2 * 148 ) : ntiles;
+    k_phasespace<<< grid, 256, p.smem ? smem : 0, st >>>( sp, sps, runs, p, out );
     return cudaGetLastError();
 }
 

@@ -166,4 +166,9 @@ __device__ __forceinline__ int cell_y( uint32_t c ) { return static_cast<int>( s
 // Work item of the particle kernels: species, tile, chunk
 struct Item { int sp; int tile; int chunk; int pad; };
 
+// Phase-space deposit parameters (quantities 0 x, 1 y, 2 ux, 3 uy, 4 uz;
+// q1 < 0 for a 1D phase space).  r = lower range bound in deposit units,
+// rdx = bins per unit, norm = weight of one particle.
+struct PhaSpec { int q0, q1, n0, n1; float r0, rdx0, r1, rdx1, norm; int smem; };
+
 }  // namespace zb

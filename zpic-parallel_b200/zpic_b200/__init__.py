@@ -39,6 +39,7 @@ EXPORTS = [
     'zpic_b200_sim_iter', 'zpic_b200_sim_nmove', 'zpic_b200_sim_synchronize', 'zpic_b200_sim_set_option',
     'zpic_b200_sim_phase_times', 'zpic_b200_sim_reset_phase_times', 'zpic_b200_sim_launch_count',
     'zpic_b200_sim_stream',
+    'zpic_b200_batch_stream', 'zpic_b200_batch_launch_count',
     'zpic_b200_emf_set_bc', 'zpic_b200_emf_advance', 'zpic_b200_emf_energy', 'zpic_b200_laser_add',
     'zpic_b200_current_set_bc', 'zpic_b200_current_set_filter', 'zpic_b200_current_zero',
     'zpic_b200_current_advance',
@@ -47,7 +48,7 @@ EXPORTS = [
     'zpic_b200_species_set_bc', 'zpic_b200_species_set_push_type', 'zpic_b200_species_energy',
     'zpic_b200_species_nmove', 'zpic_b200_species_np_total', 'zpic_b200_species_np_max_tile',
     'zpic_b200_species_get_tiles', 'zpic_b200_species_get', 'zpic_b200_species_set',
-    'zpic_b200_species_gather', 'zpic_b200_species_charge',
+    'zpic_b200_species_gather', 'zpic_b200_species_charge', 'zpic_b200_species_phasespace',
     'zpic_b200_grid_size', 'zpic_b200_grid_get', 'zpic_b200_grid_set', 'zpic_b200_grid_gather',
     'zpic_b200_batch_create', 'zpic_b200_batch_advance', 'zpic_b200_batch_synchronize',
     'zpic_b200_batch_destroy', 'zpic_b200_charge_deposit_noalloc',
@@ -114,6 +115,8 @@ def lib():
             'zpic_b200_sim_reset_phase_times': (I, [P]),
             'zpic_b200_sim_launch_count': (I, [P, U64P]),
             'zpic_b200_sim_stream': (I, [P, ctypes.POINTER(P)]),
+            'zpic_b200_batch_stream': (I, [P, ctypes.POINTER(P)]),
+            'zpic_b200_batch_launch_count': (I, [P, ctypes.POINTER(ctypes.c_uint64)]),
             'zpic_b200_emf_set_bc': (I, [P, IP]),
             'zpic_b200_emf_advance': (I, [P, I]),
             'zpic_b200_emf_energy': (I, [P, DP, DP]),
@@ -139,6 +142,7 @@ def lib():
             'zpic_b200_species_set': (I, [P, I, IP, IP, FP, FP]),
             'zpic_b200_species_gather': (I, [P, I, I, FP]),
             'zpic_b200_species_charge': (I, [P, I, FP]),
+            'zpic_b200_species_phasespace': (I, [P, I, I, FP, I, I, FP, I, FP]),
             'zpic_b200_grid_size': (I, [P, I, U64P]),
             'zpic_b200_grid_get': (I, [P, I, FP]),
             'zpic_b200_grid_set': (I, [P, I, FP]),
@@ -401,6 +405,21 @@ class Simulation:
         _check(lib().zpic_b200_species_charge(self.h, sp, _fptr(out)))
         return out
 
+    PHASESPACE = {'x': 0, 'y': 1, 'ux': 2, 'uy': 3, 'uz': 4}
+
+    def phasespace(self, sp, q0, range0, size0, q1=-1, range1=(0.0, 1.0), size1=1):
+        """Species::dep_phasespace: float32 out[size0], or out[size1, size0]
+        for a 2D phase space (q1 > q0).  Quantities by index (0 x, 1 y, 2 ux,
+        3 uy, 4 uz) or name."""
+        q0 = self.PHASESPACE.get(q0, q0)
+        q1 = self.PHASESPACE.get(q1, q1)
+        r0 = (ctypes.c_float * 2)(*range0)
+        r1 = (ctypes.c_float * 2)(*range1)
+        out = np.zeros((size0,) if q1 < 0 else (size1, size0), np.float32)
+        _check(lib().zpic_b200_species_phasespace(self.h, sp, int(q0), r0, int(size0), int(q1), r1,
+                                                  int(size1), _fptr(out)))
+        return out
+
     # ---- instrumentation ----
     def phase_times(self):
         ms = (ctypes.c_double * 5)()
@@ -439,6 +458,17 @@ class Batch:
 
     def synchronize(self):
         _check(lib().zpic_b200_batch_synchronize(self.h))
+
+    def launch_count(self):
+        v = ctypes.c_uint64()
+        _check(lib().zpic_b200_batch_launch_count(self.h, ctypes.byref(v)))
+        return v.value
+
+    def stream_handle(self):
+        """The cudaStream_t (as an int) the batch's steps run on."""
+        v = ctypes.c_void_p()
+        _check(lib().zpic_b200_batch_stream(self.h, ctypes.byref(v)))
+        return v.value or 0
 
     def close(self):
         if getattr(self, 'h', None):
