@@ -52,6 +52,7 @@ def workload_config(ncell=NCELL):
         'workload': 'uniform warm plasma %dx%d cells, 16x16 tiles, 8x8 ppc, uth 0.05, periodic' % (ncell, ncell),
         'cells': ncell * ncell, 'particles': ncell * ncell * PPC * PPC, 'tile': [TILE, TILE],
         'dx': DX, 'dt': DT, 'species': 1,
+        'current_accumulation': 'fixed point in shared memory (option jacc 2, default)',
         'l2': 'inputs larger than L2 (particle state %.1f GB)' % (ncell * ncell * PPC * PPC * 24 / 1e9),
     }
 
@@ -447,9 +448,58 @@ def run_ensemble(args, world, rank, local):
     return 0
 
 
+def run_lwfa(args, world, rank, local):
+    """Laser wakefield with a moving window: 4096x512 cells, dx 0.025, dy 0.1,
+    dt 0.022, 16x16 tiles, electrons 4x2 ppc behind a density step at x = 20,
+    cold; Gaussian pulse a0 2, omega0 10, W0 4, fwhm 2 (start 17, focus 20,
+    axis 25.6, Ez polarisation); no current filter.  Every step is one
+    Simulation::advance_mov_window from t = 0 (the window moves 0.88 cells per
+    step, injecting a new column at the right edge).  Metric: particle pushes
+    per second over the whole run, timed on the device."""
+    import torch
+    import zpic_b200 as zb
+    torch.cuda.set_device(local)
+    nx, ny = 4096, 512
+    s = zb.Simulation((nx // TILE, ny // TILE), (TILE, TILE), (nx * 0.025, ny * 0.1), 0.022, device=local)
+    s.add_species(-1.0, (4, 2), density=('step', 1.0, 20.0, 0))
+    s.add_laser('gaussian', start=17.0, fwhm=2.0, a0=2.0, omega0=10.0, W0=4.0, focus=20.0, axis=25.6, sin_pol=1)
+    s.set_moving_window()
+    np0 = s.np_total(0)
+    stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
+    steps = args.steps if args.steps_given else 2000
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    l0, n0 = s.launch_count(), s.nmove()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        s.advance_mov_window(steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
+    pushes = s.nmove() - n0
+    e, b = s.emf_energy()
+    if rank == 0:
+        print(json.dumps({
+            'metric': METRIC, 'value': pushes * world / t, 'unit': UNIT, 'n_gpus': world,
+            'steps': steps, 'warmup': 0, 'ms_per_step': t / steps * 1e3, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+            'data': 'synthetic (step density, Gaussian laser, from t = 0)',
+            'config': {'workload': 'laser wakefield, moving window, 4096x512 cells, 16x16 tiles, 4x2 ppc, '
+                                   'a0 2, %d steps from t = 0' % steps,
+                       'particles_initial': np0, 'particles_final': s.np_total(0)},
+            'cell_updates_per_second': nx * ny * steps * world / t,
+            'gpu_launches': s.launch_count() - l0,
+            'field_energy_final': float(e.sum() + b.sum()),
+            'clocks': clk.summary(),
+        }))
+    s.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--workload', default='plasma', choices=['plasma', 'ensemble'])
+    ap.add_argument('--workload', default='plasma', choices=['plasma', 'ensemble', 'lwfa'])
     ap.add_argument('--runs', type=int, default=256, help='ensemble runs (--workload ensemble)')
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=20)
@@ -460,6 +510,7 @@ def main():
     ap.add_argument('--ref-steps', type=int, default=10)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     args = ap.parse_args()
+    args.steps_given = any(a.startswith('--steps') for a in sys.argv[1:])
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup(args)
     try:
@@ -467,6 +518,8 @@ def main():
             rc = run_reference(args, world, rank)
         elif args.workload == 'ensemble':
             rc = run_ensemble(args, world, rank, local)
+        elif args.workload == 'lwfa':
+            rc = run_lwfa(args, world, rank, local)
         else:
             rc = run_gpu(args, world, rank, local)
     finally:

@@ -149,7 +149,12 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  *   "graph"          1/0  capture repeated steps in a CUDA graph (default 1)
  *   "chunks"         n    CTAs per tile in the particle kernel (0 = automatic)
  *   "profile"        1/0  record CUDA events around each kernel phase
- *   "jacc"           0/1  tile current accumulation: 0 FP32 (reference), 1 FP64
+ *   "jacc"           0/1/2 tile current accumulation in shared memory: 0 FP32
+ *                         atomics (the reference's FP32 sums, in another order),
+ *                         1 FP64 atomics, 2 fixed point (default: the FP32
+ *                         contributions rounded to 2^-29 |q| and summed exactly
+ *                         in integer arithmetic, independent of the order of
+ *                         the additions; the fastest of the three)
  */
 int zpic_b200_sim_set_option( zpic_sim * sim, const char * key, double value );
 /* Per-phase device time (ms) and launch counts accumulated while "profile" is on.

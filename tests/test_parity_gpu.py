@@ -87,6 +87,20 @@ def test_move_deposit():
     assert rel_err(g.grid('J')[:, m], o.grid('J')[:, m]) <= J_TOL
 
 
+def test_move_deposit_fp32_tile_current():
+    """Option "jacc" 0: FP32 shared atomics (the reference's FP32 sums in
+    another order)."""
+    o, g = pair(weibel)
+    g.set_option('jacc', 0)
+    for s in (o, g):
+        s.current_zero()
+    for sp in range(2):
+        o.species_move(sp)
+        g.species_move(sp)
+    m = interior_mask(o)
+    assert rel_err(g.grid('J')[:, m], o.grid('J')[:, m]) <= J_TOL
+
+
 def test_move_deposit_fp64_tile_current():
     """Option "jacc": the tile current is summed in FP64 and rounded once per
     cell; positions stay bit-exact and the current within the FP32 bar."""
@@ -101,6 +115,33 @@ def test_move_deposit_fp64_tile_current():
         assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]), 'positions differ'
     m = interior_mask(o)
     assert rel_err(g.grid('J')[:, m], o.grid('J')[:, m]) <= J_TOL
+
+
+def test_move_deposit_fixed_point_tile_current():
+    """Option "jacc" 2: 64-bit fixed-point tile current.  Positions bit-exact,
+    current within the FP32 bar, and with one CTA per tile and two species
+    (two FP32 additions per cell onto zero, which commute) the deposited
+    current is the same bit for bit on every run."""
+    o = weibel(OracleSim(*WEIBEL))
+    o.current_zero()
+    for sp in range(2):
+        o.species_move(sp)
+    runs = []
+    for _ in range(2):
+        g = weibel(zb.Simulation(*WEIBEL))
+        g.set_option('jacc', 2)
+        g.set_option('chunks', 1)
+        g.current_zero()
+        for sp in range(2):
+            g.species_move(sp)
+            a, b = o.particles(sp), g.particles(sp)
+            assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]), 'positions differ'
+        runs.append(g.grid('J'))
+    m = interior_mask(o)
+    assert rel_err(runs[0][:, m], o.grid('J')[:, m]) <= J_TOL
+    assert np.array_equal(runs[0], runs[1])
+    with pytest.raises(zb.ZpicError):
+        g.set_option('jacc', 3)
 
 
 def test_tile_sort_multisets():

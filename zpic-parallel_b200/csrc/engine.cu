@@ -29,7 +29,7 @@ struct InjRule {
 size_t particle_smem_bytes( int tile_vol, int jacc );
 size_t yee_smem_bytes( int tile_vol );
 cudaError_t launch_particles( cudaStream_t, int, int, int, const Item *, int, const SpDev *, const RunDev *, const int *,
-                              int, int );
+                              int, int, int );
 cudaError_t launch_sort( cudaStream_t, const Item *, int, const SpDev *, const int *, int, const RunDev *, int );
 cudaError_t launch_inject( cudaStream_t, int, int, const SpDev *, const RunDev *, const InjRule &, int );
 cudaError_t launch_pack( cudaStream_t, int, int, const SpDev *, const int *, int2 *, float2 *, float * );
@@ -125,7 +125,7 @@ struct HSpecies {
     void free_all() {
         PartArrays * arrs[3] = { &d.A, &d.B, &d.S };
         for ( auto * a : arrs ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
-        dfree( d.np ); dfree( d.off ); dfree( d.cap ); dfree( d.npt ); dfree( d.nidx ); dfree( d.idx );
+        dfree( d.np ); dfree( d.off ); dfree( d.cap ); dfree( d.nidx ); dfree( d.idx );
         dfree( d.aux ); dfree( d.aux2 ); dfree( d.in_cnt ); dfree( d.stage_off ); dfree( d.stage_cnt );
         dfree( d.new_off ); dfree( d.new_cap ); dfree( d.new_np ); dfree( d.extra ); dfree( d.mode );
         dfree( d.energy ); dfree( d.nmove );
@@ -157,7 +157,8 @@ struct Plan {
     std::vector<int> sp_k1_off, sp_k1_n, sp_sort_off, sp_sort_n;
     TileItem * tile_items_d = nullptr; int n_tiles = 0;
     int max_tile_vol = 0;
-    int jacc = 0;                   // FP64 tile current accumulation
+    int jacc = 0;                   // tile current accumulation (option "jacc")
+    int tile_n = 0;                 // n when every run has n x n tiles with a specialised kernel
     bool needs_bc_or_filter = false;
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
@@ -201,7 +202,7 @@ struct zpic_sim {
     // options
     bool use_graph = true;
     int chunks_opt = 0;
-    int jacc = 0;
+    int jacc = 2;                   // fixed-point tile current (option "jacc")
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[PH_N];
     double phase_ms[PH_N] = { 0 };
@@ -272,7 +273,8 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims ) {
     P.sps_h.clear(); P.sp_sim.clear(); P.sp_local.clear();
     P.sp_k1_off.clear(); P.sp_k1_n.clear(); P.sp_sort_off.clear(); P.sp_sort_n.clear();
     P.max_tile_vol = 0;
-    P.jacc = 0;
+    P.jacc = -1;
+    P.tile_n = -1;
     P.needs_bc_or_filter = false;
     int total_tiles = 0;
     for ( auto * s : sims ) for ( auto * sp : s->species ) { (void) sp; total_tiles += s->ntx * s->nty; }
@@ -283,7 +285,10 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims ) {
         zpic_sim * s = sims[r];
         runs.push_back( s->run );
         P.max_tile_vol = std::max( P.max_tile_vol, s->run.tile_vol );
-        P.jacc = std::max( P.jacc, s->jacc );
+        // one accumulation mode per plan: the runs' own when they agree
+        P.jacc = ( P.jacc < 0 || P.jacc == s->jacc ) ? s->jacc : 2;
+        const int tn = ( s->nxx == 16 && s->nxy == 16 ) ? 16 : 0;
+        P.tile_n = ( P.tile_n < 0 || P.tile_n == tn ) ? tn : 0;
         for ( int t = 0; t < s->ntx * s->nty; t++ ) tiles.push_back( { (int) r, t } );
         for ( int k = 0; k < 4; k++ )
             if ( s->emf_bc[k] > ZPIC_EMF_BC_PERIODIC || s->cur_bc[k] > ZPIC_CURRENT_BC_PERIODIC ) P.needs_bc_or_filter = true;
@@ -381,7 +386,7 @@ static int run_particles( Plan & P, cudaStream_t st, int push, int move, const i
         if ( P.n_k1[p] == 0 ) continue;
         PhaseScope ps( prof_sim( P ), st, PH_PARTICLES, 1 );
         CK( launch_particles( st, push ? p + 1 : 0, move, 1, P.k1_items_d[p], P.n_k1[p], P.sps_d, P.runs_d, shifts, P.max_tile_vol,
-                              P.jacc ) );
+                              P.jacc, P.tile_n ) );
     }
     return ZPIC_OK;
 }
@@ -604,7 +609,7 @@ static int species_upload( zpic_sim * s, HSpecies * sp, const std::vector<int> &
     CK( cudaMemcpyAsync( one, &sp->d, sizeof( SpDev ), cudaMemcpyHostToDevice, st ) );
     CK( launch_unpack( st, 0, nt, one, poff_d, ix_d, x_d, u_d ) );
     s->launches++;
-    CK( cudaMemsetAsync( sp->d.npt, 0, 9 * nt * sizeof( int ), st ) );
+    CK( cudaMemsetAsync( sp->d.in_cnt, 0, nt * sizeof( int ), st ) );
     CK( cudaMemsetAsync( sp->d.nidx, 0, nt * sizeof( int ), st ) );
     CK( cudaStreamSynchronize( st ) );
     dfree( one ); dfree( poff_d ); dfree( ix_d ); dfree( x_d ); dfree( u_d );
@@ -626,7 +631,7 @@ static int species_alloc( zpic_sim * s, HSpecies * sp, uint64_t max_part ) {
     TRY( alloc_arrays( d.B, max_part ) );
     TRY( alloc_arrays( d.S, d.stage_cap ) );
     TRY( dalloc( &d.np, nt ) ); TRY( dalloc( &d.off, nt ) ); TRY( dalloc( &d.cap, nt ) );
-    TRY( dalloc( &d.npt, 9 * nt ) ); TRY( dalloc( &d.nidx, nt ) );
+    TRY( dalloc( &d.nidx, nt ) );
     TRY( dalloc( &d.idx, max_part ) ); TRY( dalloc( &d.aux, max_part ) ); TRY( dalloc( &d.aux2, max_part ) );
     TRY( dalloc( &d.in_cnt, nt ) ); TRY( dalloc( &d.stage_off, nt ) ); TRY( dalloc( &d.stage_cnt, nt ) );
     TRY( dalloc( &d.new_off, nt ) ); TRY( dalloc( &d.new_cap, nt ) ); TRY( dalloc( &d.new_np, nt ) );
@@ -644,6 +649,15 @@ static void species_params( zpic_sim * s, HSpecies * sp ) {
     d.dt_dx = sp->dt / sp->dx[0]; d.dt_dy = sp->dt / sp->dx[1];
     d.q = sp->q;
     d.qnx = sp->q * sp->dx[0] / sp->dt; d.qny = sp->q * sp->dx[1] / sp->dt;
+    {
+        // Every current contribution of one particle segment is bounded by
+        // 1.25 |q| (|v| < c, shape weights <= 1), so with |q| < 2^e the
+        // fixed-point scale 2^(30-e) keeps it below 2^31 in magnitude.
+        int e = 0;
+        if ( sp->q != 0.0f ) std::frexp( std::fabs( sp->q ), &e );
+        d.jscale = std::ldexp( 1.0f, 30 - e );
+        d.jscale_inv = std::ldexp( 1.0, e - 30 );
+    }
     d.perx = sp->bc[0] == ZPIC_SPECIES_BC_PERIODIC;
     d.pery = sp->bc[2] == ZPIC_SPECIES_BC_PERIODIC;
     for ( int k = 0; k < 4; k++ ) d.bc[k] = sp->bc[k];
@@ -689,7 +703,7 @@ static int species_kernel( zpic_sim * s, int sp, int push, int move, const int *
     TRY( ensure_plan( s ) );
     HSpecies * h = s->species[sp];
     if ( h->counters_dirty && move ) {
-        CK( cudaMemsetAsync( h->d.npt, 0, 9 * h->ntiles * sizeof( int ), s->stream ) );
+        CK( cudaMemsetAsync( h->d.in_cnt, 0, h->ntiles * sizeof( int ), s->stream ) );
         CK( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
     }
     Plan & P = s->plan;
@@ -697,7 +711,7 @@ static int species_kernel( zpic_sim * s, int sp, int push, int move, const int *
         PhaseScope ps( s, s->stream, PH_PARTICLES, 1 );
         CK( launch_particles( s->stream, push ? 1 + h->push_type : 0, move, move ? 1 : 0,
                               P.spk1_d + P.sp_k1_off[sp], P.sp_k1_n[sp], P.sps_d, P.runs_d, shifts, P.max_tile_vol,
-                              P.jacc ) );
+                              P.jacc, P.tile_n ) );
     }
     if ( move ) { h->sort_pending = true; h->counters_dirty = true; }
     if ( push ) h->energy_items = h->ntiles * P.sps_h[sp].nchunk;
@@ -711,11 +725,11 @@ static int species_sort( zpic_sim * s, int sp, int use_extra ) {
     Plan & P = s->plan;
     if ( !h->sort_pending ) {
         // leaver lists are stale: detect them now (bnd_check, particles.cpp:212-303)
-        CK( cudaMemsetAsync( h->d.npt, 0, 9 * h->ntiles * sizeof( int ), s->stream ) );
+        CK( cudaMemsetAsync( h->d.in_cnt, 0, h->ntiles * sizeof( int ), s->stream ) );
         CK( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
         PhaseScope ps( s, s->stream, PH_SORT, 1 );
         CK( launch_particles( s->stream, 0, 0, 1, P.spk1_d + P.sp_k1_off[sp], P.sp_k1_n[sp], P.sps_d, P.runs_d,
-                              nullptr, P.max_tile_vol, 0 ) );
+                              nullptr, P.max_tile_vol, 0, 0 ) );
     }
     {
         PhaseScope ps( s, s->stream, PH_SORT, 3 );
@@ -952,7 +966,8 @@ int zpic_b200_sim_set_option( zpic_sim * s, const char * key, double v ) {
     if ( k == "graph" ) { s->use_graph = v != 0; }
     else if ( k == "profile" ) { s->profile = v != 0; if ( s->profile ) s->use_graph = false; }
     else if ( k == "jacc" ) {
-        const int j = v != 0 ? 1 : 0;
+        const int j = (int) v;
+        if ( j < 0 || j > 2 || j != v ) return fail( ZPIC_E_INVALID, "jacc must be 0, 1 or 2" );
         if ( j != s->jacc ) { s->jacc = j; s->plan.release(); }
     }
     else if ( k == "chunks" ) {
@@ -974,7 +989,7 @@ int zpic_b200_sim_advance( zpic_sim * s, int32_t nsteps ) {
     // pending fine-grained work must not be mixed with a full step
     for ( auto * sp : s->species ) {
         if ( sp->counters_dirty ) {
-            CK( cudaMemsetAsync( sp->d.npt, 0, 9 * sp->ntiles * sizeof( int ), s->stream ) );
+            CK( cudaMemsetAsync( sp->d.in_cnt, 0, sp->ntiles * sizeof( int ), s->stream ) );
             CK( cudaMemsetAsync( sp->d.nidx, 0, sp->ntiles * sizeof( int ), s->stream ) );
             sp->counters_dirty = false;
         }
@@ -1484,7 +1499,7 @@ int zpic_b200_batch_advance( zpic_batch * b, int32_t nsteps ) {
         CK( cudaStreamWaitEvent( b->stream, b->ev, 0 ) );
         for ( auto * sp : s->species )
             if ( sp->counters_dirty ) {
-                CK( cudaMemsetAsync( sp->d.npt, 0, 9 * sp->ntiles * sizeof( int ), b->stream ) );
+                CK( cudaMemsetAsync( sp->d.in_cnt, 0, sp->ntiles * sizeof( int ), b->stream ) );
                 CK( cudaMemsetAsync( sp->d.nidx, 0, sp->ntiles * sizeof( int ), b->stream ) );
                 sp->counters_dirty = false;
             }

@@ -8,6 +8,7 @@
 #include "zpic_dev.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace zb {
 
@@ -111,11 +112,33 @@ __device__ __forceinline__ void dudt_boris_euler( float alpha, float ex, float e
     uz = __fmaf_rn( r13, utx, __fmaf_rn( r23, uty, r33 * utz ) ) + ez;
 }
 
+// Accumulation of one current contribution into the shared-memory tile
+// current: FP32 or FP64 atomics, or fixed point.  Fixed point: the
+// contribution times js (a power of two that keeps every contribution below
+// 2^31 in magnitude) is rounded to an integer x = hi * 2^16 + lo, and hi
+// (signed) and lo (0..65535) are added to two 32-bit integer accumulators
+// with native shared-memory integer atomics; the lo words sit jlo entries
+// after the hi words.  Integer sums do not depend on the order of the
+// additions; hi and lo sums cannot overflow for up to 2^16 additions per
+// entry, and the kernel flushes the accumulators before that many.
+struct JAcc { float js; int jlo; };
+__device__ __forceinline__ void jadd( float * p, float v, JAcc ) { atomicAdd( p, v ); }
+__device__ __forceinline__ void jadd( double * p, float v, JAcc ) { atomicAdd( p, (double) v ); }
+__device__ __forceinline__ void jadd( int * p, float v, JAcc a ) {
+    const int x = __float2int_rn( v * a.js );
+    atomicAdd( p, x >> 16 );
+    atomicAdd( reinterpret_cast<unsigned int *>( p + a.jlo ), (unsigned int) ( x & 0xFFFF ) );
+}
+// value of a fixed-point accumulator pair
+__device__ __forceinline__ double jfix_value( int hi, unsigned int lo, double inv ) {
+    return ( (double) hi * 65536.0 + (double) lo ) * inv;
+}
+
 // Charge-conserving current of one segment inside one cell (species.cpp:267-310),
 // accumulated into the shared-memory tile current with shared atomics.
 template < typename JT >
 __device__ __forceinline__ void dep_current_seg( int ix, int iy, float x0x, float x0y, float x1x, float x1y,
-                                                 float qnxx, float qnxy, float qvz, JT * J, int stride ) {
+                                                 float qnxx, float qnxy, float qvz, JT * J, int stride, JAcc ja ) {
     const float S0x0 = 0.5f - x0x, S0x1 = 0.5f + x0x;
     const float S1x0 = 0.5f - x1x, S1x1 = 0.5f + x1x;
     const float S0y0 = 0.5f - x0y, S0y1 = 0.5f + x0y;
@@ -126,14 +149,14 @@ __device__ __forceinline__ void dep_current_seg( int ix, int iy, float x0x, floa
     const float wp20 = 0.5f * ( S0x0 + S1x0 ), wp21 = 0.5f * ( S0x1 + S1x1 );
     JT * Js = J + 3 * ( ix + stride * iy );
     const int s3 = 3 * stride;
-    atomicAdd( Js + 0,      (JT) ( wl1 * wp10 ) );
-    atomicAdd( Js + 1,      (JT) ( wl2 * wp20 ) );
-    atomicAdd( Js + 2,      (JT) ( qvz * ( S0x0 * S0y0 + S1x0 * S1y0 + ( S0x0 * S1y0 - S1x0 * S0y0 ) / 2.0f ) ) );
-    atomicAdd( Js + 3 + 1,  (JT) ( wl2 * wp21 ) );
-    atomicAdd( Js + 3 + 2,  (JT) ( qvz * ( S0x1 * S0y0 + S1x1 * S1y0 + ( S0x1 * S1y0 - S1x1 * S0y0 ) / 2.0f ) ) );
-    atomicAdd( Js + s3 + 0, (JT) ( wl1 * wp11 ) );
-    atomicAdd( Js + s3 + 2, (JT) ( qvz * ( S0x0 * S0y1 + S1x0 * S1y1 + ( S0x0 * S1y1 - S1x0 * S0y1 ) / 2.0f ) ) );
-    atomicAdd( Js + s3 + 5, (JT) ( qvz * ( S0x1 * S0y1 + S1x1 * S1y1 + ( S0x1 * S1y1 - S1x1 * S0y1 ) / 2.0f ) ) );
+    jadd( Js + 0,      wl1 * wp10, ja );
+    jadd( Js + 1,      wl2 * wp20, ja );
+    jadd( Js + 2,      qvz * ( S0x0 * S0y0 + S1x0 * S1y0 + ( S0x0 * S1y0 - S1x0 * S0y0 ) / 2.0f ), ja );
+    jadd( Js + 3 + 1,  wl2 * wp21, ja );
+    jadd( Js + 3 + 2,  qvz * ( S0x1 * S0y0 + S1x1 * S1y0 + ( S0x1 * S1y0 - S1x1 * S0y0 ) / 2.0f ), ja );
+    jadd( Js + s3 + 0, wl1 * wp11, ja );
+    jadd( Js + s3 + 2, qvz * ( S0x0 * S0y1 + S1x0 * S1y1 + ( S0x0 * S1y1 - S1x0 * S0y1 ) / 2.0f ), ja );
+    jadd( Js + s3 + 5, qvz * ( S0x1 * S0y1 + S1x1 * S1y1 + ( S0x1 * S1y1 - S1x1 * S0y1 ) / 2.0f ), ja );
 }
 
 // Split the trajectory of a particle that crosses at least one cell edge into
@@ -142,7 +165,7 @@ __device__ __forceinline__ void dep_current_seg( int ix, int iy, float x0x, floa
 template < typename JT >
 __device__ __forceinline__ void deposit_crossing( int ix, int iy, float x0x, float x0y, float x1x, float x1y,
                                                   float dx, float dy, float qvz, float qnxx, float qnxy,
-                                                  JT * J, int stride ) {
+                                                  JT * J, int stride, JAcc ja ) {
     const int dix = ( ( x1x >= 0.5f ) - ( x1x < -0.5f ) );
     const int diy = ( ( x1y >= 0.5f ) - ( x1y < -0.5f ) );
     const int crossx = dix != 0, crossy = diy != 0;
@@ -194,9 +217,9 @@ __device__ __forceinline__ void deposit_crossing( int ix, int iy, float x0x, flo
             }
         }
     }
-    dep_current_seg( v0x, v0y, v0x0, v0y0, v0x1, v0y1, qnxx, qnxy, v0q, J, stride );
-    dep_current_seg( v1x, v1y, v1x0, v1y0, v1x1, v1y1, qnxx, qnxy, v1q, J, stride );
-    if ( crossx && crossy ) dep_current_seg( v2x, v2y, v2x0, v2y0, v2x1, v2y1, qnxx, qnxy, v2q, J, stride );
+    dep_current_seg( v0x, v0y, v0x0, v0y0, v0x1, v0y1, qnxx, qnxy, v0q, J, stride, ja );
+    dep_current_seg( v1x, v1y, v1x0, v1y0, v1x1, v1y1, qnxx, qnxy, v1q, J, stride, ja );
+    if ( crossx && crossy ) dep_current_seg( v2x, v2y, v2x0, v2y0, v2x1, v2y1, qnxx, qnxy, v2q, J, stride, ja );
 }
 
 // Per-warp ring of cell-crossing particles waiting for their split deposit.
@@ -207,10 +230,11 @@ struct CrossQueue {
 };
 
 template < typename JT >
-__device__ __forceinline__ void drain_entry( const CrossQueue & Q, int e, float qnxx, float qnxy, JT * J, int stride ) {
+__device__ __forceinline__ void drain_entry( const CrossQueue & Q, int e, float qnxx, float qnxy, JT * J, int stride,
+                                             JAcc ja ) {
     const uint32_t c = Q.cell[e];
     const float x0x = Q.x0x[e], x0y = Q.x0y[e], dx = Q.dx[e], dy = Q.dy[e];
-    deposit_crossing( cell_x( c ), cell_y( c ), x0x, x0y, x0x + dx, x0y + dy, dx, dy, Q.qvz[e], qnxx, qnxy, J, stride );
+    deposit_crossing( cell_x( c ), cell_y( c ), x0x, x0y, x0x + dx, x0y + dy, dx, dy, Q.qvz[e], qnxx, qnxy, J, stride, ja );
 }
 
 // ---------------------------------------------------------------------------
@@ -233,13 +257,24 @@ __device__ __forceinline__ void drain_entry( const CrossQueue & Q, int e, float 
 // that cross a cell edge are queued per warp and split/deposited in full-warp
 // passes, so the two- and three-segment code runs without divergence.
 // ---------------------------------------------------------------------------
+// Target tile index along one axis for a particle leaving through v (periodic
+// wrap, or -1 past an open edge).
+__device__ __forceinline__ int wrap_tile( int v, int n, int periodic ) {
+    if ( periodic ) { if ( v < 0 ) v += n; if ( v >= n ) v -= n; return v; }
+    return ( v >= 0 && v < n ) ? v : -1;
+}
+
 constexpr int PK_THREADS = 256;
 constexpr int PK_PPT = 2;                   // particles per thread per block iteration
 
 // JT is the type of the tile current accumulated in shared memory: float
-// (the reference's FP32 sums) or double (FP64 accumulation, rounded to FP32
-// once per cell when the tile is added to the global deposit buffer).
-template < int PUSH, int MOVE, bool DETECT, typename JT = float >
+// (FP32 sums, as the reference), double (FP64 sums) or int (fixed point in
+// two 32-bit words, order-independent); the last two are rounded
+// to FP32 once per cell when the tile is added to the global deposit buffer.
+// TN > 0 fixes square TN x TN tiles at compile time, so every shared-memory
+// offset of the interpolation and deposit stencils is an immediate; TN = 0
+// reads the tile shape from the run descriptor.
+template < int PUSH, int MOVE, bool DETECT, typename JT = float, int TN = 0 >
 __global__ void __launch_bounds__( PK_THREADS, 4 )
 k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
              const RunDev * __restrict__ runs, const int * __restrict__ shifts )
@@ -248,16 +283,18 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     const Item it = items[ blockIdx.x ];
     const SpDev & S = sps[ it.sp ];
     const RunDev & R = runs[ S.run ];
-    const int tv = R.tile_vol;
+    const int tv = TN ? ( ( ( TN + 3 ) * ( TN + 3 ) + 3 ) & ~3 ) : R.tile_vol;
     const int t = it.tile;
     const int nchunk = S.nchunk;
 
-    // shared memory: [E tile][B tile][tile current (JT)][mbarrier]
-    //                [energy partials][crossing queues]
+    // shared memory: [E tile][B tile][tile current (JT; fixed point: hi
+    //                words then lo words)][mbarrier][energy partials][crossing queues]
+    constexpr bool FIX = std::is_same<JT, int>::value;
+    constexpr int JW = FIX ? 2 : 1;
     float * sE = reinterpret_cast<float *>( smem_raw );
     float * sB = sE + 3 * tv;
     JT * sJ = reinterpret_cast<JT *>( sB + 3 * tv );
-    uint64_t * bar = reinterpret_cast<uint64_t *>( sJ + 3 * tv );
+    uint64_t * bar = reinterpret_cast<uint64_t *>( sJ + 3 * tv * JW );
     double * sred = reinterpret_cast<double *>( bar + 1 );
     CrossQueue * xq = reinterpret_cast<CrossQueue *>( sred + PK_THREADS / 32 );
 
@@ -287,16 +324,17 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
         }
     }
     if ( MOVE == 2 ) {
-        for ( int i = threadIdx.x; i < 3 * tv; i += blockDim.x ) sJ[i] = (JT) 0;
+        for ( int i = threadIdx.x; i < 3 * tv * JW; i += blockDim.x ) sJ[i] = (JT) 0;
     }
     if ( PUSH ) mbar_wait_bounded( bar, 0, R.status );
     __syncthreads();
 
-    const int ys = R.extx;
-    const float * Ec = sE + 3 * R.gc_off;
-    const float * Bc = sB + 3 * R.gc_off;
-    JT * Jc = sJ + 3 * R.gc_off;
-    const int nxx = R.nxx, nxy = R.nxy;
+    const int ys = TN ? TN + 3 : R.extx;
+    const int gc_off = TN ? TN + 4 : R.gc_off;
+    const float * Ec = sE + 3 * gc_off;
+    const float * Bc = sB + 3 * gc_off;
+    JT * Jc = sJ + 3 * gc_off;
+    const int nxx = TN ? TN : R.nxx, nxy = TN ? TN : R.nxy;
     const int tx = t % R.ntx, ty = t / R.ntx;
     const int shift = ( MOVE && shifts ) ? shifts[ it.sp ] : 0;
     const bool euler = ( PUSH == 2 );
@@ -310,6 +348,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
 
     const float alpha = S.alpha;
     const float dt_dx = S.dt_dx, dt_dy = S.dt_dy, q = S.q, qnxx = S.qnx, qnxy = S.qny;
+    const JAcc ja = { S.jscale, 3 * tv };
 
     uint32_t * __restrict__ pc = S.A.cell + off;
     float * __restrict__ pxx = S.A.xx + off;
@@ -372,7 +411,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                         qz = q * u2[k] * rg * 0.5f;
                         cross = ( dix | diy ) != 0;
                         if ( !cross )
-                            dep_current_seg( ix, iy, x0[k], x1[k], x1x, x1y, qnxx, qnxy, qz, Jc, ys );
+                            dep_current_seg( ix, iy, x0[k], x1[k], x1x, x1y, qnxx, qnxy, qz, Jc, ys, ja );
                     }
                     ox = x0[k]; oy = x1[k]; oix = ix; oiy = iy;
                     x0[k] = x1x - dix; x1[k] = x1y - diy;
@@ -402,7 +441,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                     qt += __popc( m );
                     if ( qt - qh >= 32 ) {
                         __syncwarp();
-                        drain_entry( Q, ( qh + lane ) & ( XQ - 1 ), qnxx, qnxy, Jc, ys );
+                        drain_entry( Q, ( qh + lane ) & ( XQ - 1 ), qnxx, qnxy, Jc, ys, ja );
                         qh += 32;
                         __syncwarp();
                     }
@@ -443,15 +482,39 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                     if ( leave_dir[k] != 4 ) {
                         S.idx[ off + pos ] = b0 + k * PK_THREADS + threadIdx.x;
                         pos++;
-                        atomicAdd( S.npt + 9 * t + leave_dir[k], 1 );
+                        // incoming count of the target tile (bnd_check's
+                        // per-direction counts, summed where they are used)
+                        const int ttx = wrap_tile( tx + leave_dir[k] % 3 - 1, R.ntx, S.perx );
+                        const int tty = wrap_tile( ty + leave_dir[k] / 3 - 1, R.nty, S.pery );
+                        if ( ttx >= 0 && tty >= 0 ) atomicAdd( S.in_cnt + tty * R.ntx + ttx, 1 );
                     }
                 }
+            }
+        }
+        if constexpr ( FIX && MOVE == 2 ) {
+            // flush the fixed-point accumulators every 32 blocks (16384
+            // particles, at most 3 additions each per entry) into the raw
+            // current, before the 2^16 additions the words can take
+            if ( ( ( b0 - begin ) / ( PK_PPT * PK_THREADS ) ) % 32 == 31 && b0 + PK_PPT * PK_THREADS < end ) {
+                __syncthreads();
+                unsigned int * lo = reinterpret_cast<unsigned int *>( sJ ) + 3 * tv;
+                float * dst = R.Jdep + (size_t) t * 3 * tv;
+                for ( int i = threadIdx.x; i < 3 * tv; i += blockDim.x ) {
+                    const int h = sJ[i];
+                    const unsigned int l = lo[i];
+                    if ( h != 0 || l != 0 ) {
+                        atomicAdd( dst + i, (float) jfix_value( h, l, S.jscale_inv ) );
+                        sJ[i] = 0;
+                        lo[i] = 0;
+                    }
+                }
+                __syncthreads();
             }
         }
     }
     if ( MOVE == 2 && qt != qh ) {
         __syncwarp();
-        if ( lane < qt - qh ) drain_entry( Q, ( qh + lane ) & ( XQ - 1 ), qnxx, qnxy, Jc, ys );
+        if ( lane < qt - qh ) drain_entry( Q, ( qh + lane ) & ( XQ - 1 ), qnxx, qnxy, Jc, ys, ja );
     }
 
     if ( PUSH ) {
@@ -462,9 +525,14 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     }
     __syncthreads();
     const float * sJout = reinterpret_cast<const float *>( sJ );
-    if ( MOVE == 2 && sizeof( JT ) == 8 ) {
-        // round the FP64 tile current once per cell, into the E tile's place
-        for ( int i = threadIdx.x; i < 3 * tv; i += blockDim.x ) sE[i] = (float) sJ[i];
+    if ( MOVE == 2 && !std::is_same<JT, float>::value ) {
+        // round the FP64 or fixed-point tile current once per cell, into the E tile's place
+        for ( int i = threadIdx.x; i < 3 * tv; i += blockDim.x ) {
+            if constexpr ( FIX )
+                sE[i] = (float) jfix_value( sJ[i], reinterpret_cast<const unsigned int *>( sJ )[ 3 * tv + i ],
+                                            S.jscale_inv );
+            else sE[i] = (float) sJ[i];
+        }
         sJout = sE;
         __syncthreads();
     }
@@ -488,10 +556,6 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
 // Tile sort (particles.cpp:212-614 semantics; slot layout with slack)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ int wrap_tile( int v, int n, int periodic ) {
-    if ( periodic ) { if ( v < 0 ) v += n; if ( v >= n ) v -= n; return v; }
-    return ( v >= 0 && v < n ) ? v : -1;
-}
 
 // Block-wide exclusive scan of one value per thread; the block total is
 // written to *total (a shared variable) and visible on return.
@@ -527,9 +591,10 @@ __device__ __forceinline__ long long block_exscan( long long v, long long * tota
 
 constexpr int PLAN_THREADS = 1024;
 
-// Sort plan: one CTA per species.  Counts incoming particles per tile,
-// decides between the in-place path (everything fits its slot and the
-// staging buffer) and a repack, and lays out offsets for either.
+// Sort plan: one CTA per species.  From the incoming counts (summed by the
+// leaver detection) and the stayers of each tile it decides between the
+// in-place path (everything fits its slot and the staging buffer) and a
+// repack, and lays out offsets for either.
 __global__ void __launch_bounds__( PLAN_THREADS )
 k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_list,
              const RunDev * __restrict__ runs, int use_extra )
@@ -537,7 +602,6 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
     const SpDev & S = sps[ species_list[ blockIdx.x ] ];
     const RunDev & R = runs[ S.run ];
     const int nt = S.ntiles;
-    const int ntx = R.ntx, nty = R.nty;
     const int per = ( nt + PLAN_THREADS - 1 ) / PLAN_THREADS;
     const int t0 = min( nt, (int) threadIdx.x * per ), t1 = min( nt, t0 + per );
     __shared__ long long s_total;
@@ -548,17 +612,9 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
     long long in_sum = 0;
     int fit = 1;
     for ( int t = t0; t < t1; t++ ) {
-        const int tx = t % ntx, ty = t / ntx;
-        int in = 0;
-        for ( int d = 0; d < 9; d++ ) {
-            if ( d == 4 ) continue;
-            const int sx = wrap_tile( tx - ( d % 3 - 1 ), ntx, S.perx );
-            const int sy = wrap_tile( ty - ( d / 3 - 1 ), nty, S.pery );
-            if ( sx >= 0 && sy >= 0 ) in += S.npt[ 9 * ( sy * ntx + sx ) + d ];
-        }
+        const int in = S.in_cnt[t];
         const int stay = S.np[t] - S.nidx[t];
         const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
-        S.in_cnt[t] = in;
         S.new_np[t] = stay + in;
         S.stage_cnt[t] = 0;
         if ( stay + in + ex > S.cap[t] ) fit = 0;
@@ -623,14 +679,22 @@ __device__ __forceinline__ void copy_particle( const PartArrays & d, size_t di, 
     d.ux[di] = s.ux[si]; d.uy[di] = s.uy[si]; d.uz[di] = s.uz[si];
 }
 
-constexpr int SORT_THREADS = 128;
+constexpr int SORT_THREADS = 256;
+constexpr int SORT_WARPS = SORT_THREADS / 32;     // one tile per warp
 
 // Leavers to staging (or, when repacking, every particle to buffer B), then
-// fill the holes left in [0, n0) with the stayers found in the tail.
+// fill the holes left in [0, n0) with the stayers found in the tail.  One
+// warp per tile: the hole and stayer lists are compacted with ballots, in
+// particle order, and paired by rank.
 __global__ void __launch_bounds__( SORT_THREADS )
-k_sort_out( const Item * __restrict__ items, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs )
+k_sort_out( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps,
+            const RunDev * __restrict__ runs )
 {
-    const Item it = items[ blockIdx.x ];
+    const int wi = blockIdx.x * SORT_WARPS + ( threadIdx.x >> 5 );
+    if ( wi >= nitems ) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = ( 1u << lane ) - 1u;
+    const Item it = items[ wi ];
     const SpDev & S = sps[ it.sp ];
     const RunDev & R = runs[ S.run ];
     const int mode = *S.mode;
@@ -639,59 +703,82 @@ k_sort_out( const Item * __restrict__ items, const SpDev * __restrict__ sps, con
     const int ntx = R.ntx, nty = R.nty, nxx = R.nxx, nxy = R.nxy;
     const int tx = t % ntx, ty = t / ntx;
     const int np = S.np[t], nl = S.nidx[t], n0 = np - nl, off = S.off[t];
-    __shared__ int s_nh, s_ns;
-    if ( threadIdx.x == 0 ) { s_nh = 0; s_ns = 0; }
-    __syncthreads();
 
     if ( mode == 0 ) {
-        for ( int k = threadIdx.x; k < nl; k += blockDim.x ) {
-            const int i = S.idx[ off + k ];
-            const size_t g = (size_t) off + i;
-            const uint32_t c = S.A.cell[g];
-            int ix = cell_x( c ), iy = cell_y( c );
-            const int xc = ( ix >= nxx ) - ( ix < 0 ), yc = ( iy >= nxy ) - ( iy < 0 );
-            const int ttx = wrap_tile( tx + xc, ntx, S.perx ), tty = wrap_tile( ty + yc, nty, S.pery );
-            if ( ttx >= 0 && tty >= 0 ) {
-                const int tt = tty * ntx + ttx;
-                const int slot = atomicAdd( S.stage_cnt + tt, 1 );
-                const size_t d = (size_t) S.stage_off[tt] + slot;
-                S.S.cell[d] = pack_cell( ix - xc * nxx, iy - yc * nxy );
-                S.S.xx[d] = S.A.xx[g]; S.S.xy[d] = S.A.xy[g];
-                S.S.ux[d] = S.A.ux[g]; S.S.uy[d] = S.A.uy[g]; S.S.uz[d] = S.A.uz[g];
+        int nh = 0;
+        for ( int k0 = 0; k0 < nl; k0 += 32 ) {
+            const int k = k0 + lane;
+            bool hole = false;
+            int i = 0;
+            if ( k < nl ) {
+                i = S.idx[ off + k ];
+                const size_t g = (size_t) off + i;
+                const uint32_t c = S.A.cell[g];
+                const int ix = cell_x( c ), iy = cell_y( c );
+                const int xc = ( ix >= nxx ) - ( ix < 0 ), yc = ( iy >= nxy ) - ( iy < 0 );
+                const int ttx = wrap_tile( tx + xc, ntx, S.perx ), tty = wrap_tile( ty + yc, nty, S.pery );
+                if ( ttx >= 0 && tty >= 0 ) {
+                    const int tt = tty * ntx + ttx;
+                    const int slot = atomicAdd( S.stage_cnt + tt, 1 );
+                    const size_t d = (size_t) S.stage_off[tt] + slot;
+                    S.S.cell[d] = pack_cell( ix - xc * nxx, iy - yc * nxy );
+                    S.S.xx[d] = S.A.xx[g]; S.S.xy[d] = S.A.xy[g];
+                    S.S.ux[d] = S.A.ux[g]; S.S.uy[d] = S.A.uy[g]; S.S.uz[d] = S.A.uz[g];
+                }
+                hole = i < n0;
             }
-            if ( i < n0 ) S.aux[ off + atomicAdd( &s_nh, 1 ) ] = i;
+            const unsigned m = __ballot_sync( 0xffffffffu, hole );
+            if ( hole ) S.aux[ off + nh + __popc( m & lt ) ] = i;
+            nh += __popc( m );
         }
-        for ( int ci = n0 + threadIdx.x; ci < np; ci += blockDim.x ) {
-            const uint32_t c = S.A.cell[ (size_t) off + ci ];
-            const int ix = cell_x( c ), iy = cell_y( c );
-            if ( ix >= 0 && ix < nxx && iy >= 0 && iy < nxy ) S.aux2[ off + atomicAdd( &s_ns, 1 ) ] = ci;
+        int ns = 0;
+        for ( int c0 = n0; c0 < np; c0 += 32 ) {
+            const int ci = c0 + lane;
+            bool stay = false;
+            if ( ci < np ) {
+                const uint32_t c = S.A.cell[ (size_t) off + ci ];
+                const int ix = cell_x( c ), iy = cell_y( c );
+                stay = ix >= 0 && ix < nxx && iy >= 0 && iy < nxy;
+            }
+            const unsigned m = __ballot_sync( 0xffffffffu, stay );
+            if ( stay ) S.aux2[ off + ns + __popc( m & lt ) ] = ci;
+            ns += __popc( m );
         }
-        __syncthreads();
-        const int nh = min( s_nh, s_ns );
-        if ( threadIdx.x == 0 && s_nh != s_ns ) atomicOr( R.status, ST_BAD_CELL );
-        for ( int r = threadIdx.x; r < nh; r += blockDim.x )
+        __syncwarp();
+        const int nh2 = min( nh, ns );
+        if ( lane == 0 && nh != ns ) atomicOr( R.status, ST_BAD_CELL );
+        for ( int r = lane; r < nh2; r += 32 )
             copy_particle( S.A, (size_t) off + S.aux[ off + r ], S.A, (size_t) off + S.aux2[ off + r ] );
-        __syncthreads();
-        if ( threadIdx.x == 0 ) S.np[t] = n0;
+        __syncwarp();
+        if ( lane == 0 ) S.np[t] = n0;
     } else {
         // repack: stayers to B at new_off[t] + rank, leavers to B after the
         // target's stayers.
-        for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
-            const size_t g = (size_t) off + i;
-            const uint32_t c = S.A.cell[g];
-            const int ix = cell_x( c ), iy = cell_y( c );
-            const int xc = ( ix >= nxx ) - ( ix < 0 ), yc = ( iy >= nxy ) - ( iy < 0 );
-            if ( xc == 0 && yc == 0 ) {
-                const size_t d = (size_t) S.new_off[t] + atomicAdd( &s_ns, 1 );
-                copy_particle( S.B, d, S.A, g );
-            } else {
+        int ns = 0;
+        for ( int i0 = 0; i0 < np; i0 += 32 ) {
+            const int i = i0 + lane;
+            bool stay = false;
+            size_t g = 0;
+            uint32_t c = 0;
+            int xc = 0, yc = 0;
+            if ( i < np ) {
+                g = (size_t) off + i;
+                c = S.A.cell[g];
+                const int ix = cell_x( c ), iy = cell_y( c );
+                xc = ( ix >= nxx ) - ( ix < 0 ); yc = ( iy >= nxy ) - ( iy < 0 );
+                stay = xc == 0 && yc == 0;
+            }
+            const unsigned m = __ballot_sync( 0xffffffffu, stay );
+            if ( stay ) copy_particle( S.B, (size_t) S.new_off[t] + ns + __popc( m & lt ), S.A, g );
+            ns += __popc( m );
+            if ( i < np && !stay ) {
                 const int ttx = wrap_tile( tx + xc, ntx, S.perx ), tty = wrap_tile( ty + yc, nty, S.pery );
                 if ( ttx >= 0 && tty >= 0 ) {
                     const int tt = tty * ntx + ttx;
                     const int slot = atomicAdd( S.stage_cnt + tt, 1 );
                     const size_t d = (size_t) S.new_off[tt] + ( S.np[tt] - S.nidx[tt] ) + slot;
                     copy_particle( S.B, d, S.A, g );
-                    S.B.cell[d] = pack_cell( ix - xc * nxx, iy - yc * nxy );
+                    S.B.cell[d] = pack_cell( cell_x( c ) - xc * nxx, cell_y( c ) - yc * nxy );
                 }
             }
         }
@@ -699,29 +786,31 @@ k_sort_out( const Item * __restrict__ items, const SpDev * __restrict__ sps, con
 }
 
 // Incoming particles from staging appended after the stayers (or the
-// repacked tile copied back from B); resets the per-tile leaver counters.
+// repacked tile copied back from B); resets the per-tile counters.  One warp
+// per tile.
 __global__ void __launch_bounds__( SORT_THREADS )
-k_sort_in( const Item * __restrict__ items, const SpDev * __restrict__ sps )
+k_sort_in( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps )
 {
-    const Item it = items[ blockIdx.x ];
+    const int wi = blockIdx.x * SORT_WARPS + ( threadIdx.x >> 5 );
+    if ( wi >= nitems ) return;
+    const int lane = threadIdx.x & 31;
+    const Item it = items[ wi ];
     const SpDev & S = sps[ it.sp ];
     const int mode = *S.mode;
     const int t = it.tile;
     if ( mode == 0 ) {
         const int n0 = S.np[t], in = S.in_cnt[t], off = S.off[t], so = S.stage_off[t];
-        for ( int k = threadIdx.x; k < in; k += blockDim.x )
+        for ( int k = lane; k < in; k += 32 )
             copy_particle( S.A, (size_t) off + n0 + k, S.S, (size_t) so + k );
-        __syncthreads();
-        if ( threadIdx.x == 0 ) S.np[t] = n0 + in;
+        if ( lane == 0 ) S.np[t] = n0 + in;
     } else if ( mode == 1 ) {
         const int n = S.new_np[t], off = S.new_off[t];
-        for ( int k = threadIdx.x; k < n; k += blockDim.x )
+        for ( int k = lane; k < n; k += 32 )
             copy_particle( S.A, (size_t) off + k, S.B, (size_t) off + k );
-        __syncthreads();
-        if ( threadIdx.x == 0 ) { S.np[t] = n; S.off[t] = off; S.cap[t] = S.new_cap[t]; }
+        if ( lane == 0 ) { S.np[t] = n; S.off[t] = off; S.cap[t] = S.new_cap[t]; }
     }
-    if ( threadIdx.x < 9 ) S.npt[ 9 * t + threadIdx.x ] = 0;
-    if ( threadIdx.x == 0 ) S.nidx[t] = 0;
+    __syncwarp();
+    if ( lane == 0 ) { S.in_cnt[t] = 0; S.nidx[t] = 0; }
 }
 
 // ---------------------------------------------------------------------------
@@ -1028,11 +1117,23 @@ size_t particle_smem_bytes( int tile_vol, int jacc ) {
 
 typedef void ( *pk_fn )( const Item *, const SpDev *, const RunDev *, const int * );
 
-static pk_fn pick_particle_kernel( int push, int move, int detect, int jacc ) {
-    if ( jacc && move == 2 ) {
+static pk_fn pick_particle_kernel( int push, int move, int detect, int jacc, int tile_n ) {
+    if ( tile_n == 16 && move == 2 && detect && ( push == 1 || push == 2 ) ) {
+        if ( jacc == 0 ) return push == 1 ? k_particles< 1, 2, true, float, 16 > : k_particles< 2, 2, true, float, 16 >;
+        if ( jacc == 1 ) return push == 1 ? k_particles< 1, 2, true, double, 16 > : k_particles< 2, 2, true, double, 16 >;
+        return push == 1 ? k_particles< 1, 2, true, int, 16 >
+                         : k_particles< 2, 2, true, int, 16 >;
+    }
+    if ( jacc == 1 && move == 2 ) {
 #define PKD( P, M, D ) if ( push == P && move == M && detect == D ) return k_particles< P, M, D, double >;
         PKD( 1, 2, true ) PKD( 2, 2, true ) PKD( 0, 2, true )
 #undef PKD
+        return nullptr;
+    }
+    if ( jacc == 2 && move == 2 ) {
+#define PKX( P, M, D ) if ( push == P && move == M && detect == D ) return k_particles< P, M, D, int >;
+        PKX( 1, 2, true ) PKX( 2, 2, true ) PKX( 0, 2, true )
+#undef PKX
         return nullptr;
     }
 #define PK( P, M, D ) if ( push == P && move == M && detect == D ) return k_particles< P, M, D >;
@@ -1046,9 +1147,9 @@ static pk_fn pick_particle_kernel( int push, int move, int detect, int jacc ) {
 
 cudaError_t launch_particles( cudaStream_t st, int push, int move, int detect, const Item * items, int nitems,
                               const SpDev * sps, const RunDev * runs, const int * shifts, int max_tile_vol,
-                              int jacc ) {
-    jacc = ( jacc && move == 2 ) ? 1 : 0;
-    pk_fn f = pick_particle_kernel( push, move, detect, jacc );
+                              int jacc, int tile_n ) {
+    if ( move != 2 ) jacc = 0;
+    pk_fn f = pick_particle_kernel( push, move, detect, jacc, tile_n );
     if ( !f ) return cudaErrorInvalidValue;
     const size_t smem = particle_smem_bytes( max_tile_vol, jacc );
     if ( smem > 48 * 1024 )
@@ -1062,8 +1163,9 @@ cudaError_t launch_sort( cudaStream_t st, const Item * items, int nitems, const 
                          const int * species_list, int nspecies, const RunDev * runs, int use_extra ) {
     if ( nitems <= 0 ) return cudaSuccess;
     k_sort_plan<<< nspecies, PLAN_THREADS, 0, st >>>( sps, species_list, runs, use_extra );
-    k_sort_out<<< nitems, SORT_THREADS, 0, st >>>( items, sps, runs );
-    k_sort_in<<< nitems, SORT_THREADS, 0, st >>>( items, sps );
+    const int nb = ( nitems + SORT_WARPS - 1 ) / SORT_WARPS;
+    k_sort_out<<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, runs );
+    k_sort_in<<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps );
     return cudaGetLastError();
 }
 

@@ -57,11 +57,10 @@ struct SpDev {
     int stage_cap;                // capacity of the staging buffer
     PartArrays A, B, S;
     int * np; int * off; int * cap;          // tile slots of A
-    int * npt;                    // [ntiles*9] leavers per direction (npt[4] unused)
     int * nidx;                   // [ntiles] leavers per tile
     int * idx;                    // [max_part] local index of leavers, at off[t]+k
     int * aux; int * aux2;        // [max_part] hole / tail lists, at off[t]+k
-    int * in_cnt;                 // [ntiles] incoming particles
+    int * in_cnt;                 // [ntiles] incoming particles (counted by the leaver detection)
     int * stage_off;              // [ntiles] staging offsets (exclusive scan of in_cnt)
     int * stage_cnt;              // [ntiles] staging fill counters
     int * new_off; int * new_cap; int * new_np;  // [ntiles] repack layout
@@ -76,6 +75,8 @@ struct SpDev {
     int perx, pery;               // particle periodic flags
     int bc[4];                    // species::bc
     int min_slack;                // minimum free slots per tile after a repack
+    float jscale;                 // fixed-point tile current: 2^k with |q| * jscale < 2^30
+    double jscale_inv;            // 1 / jscale
 };
 
 // ---------------------------------------------------------------------------
