@@ -479,6 +479,12 @@ def run_lwfa(args, world, rank, local):
     t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
     pushes = s.nmove() - n0
     e, b = s.emf_energy()
+    # per-phase device time over 100 further steps (CUDA events around each phase)
+    s.set_option('profile', 1)
+    s.reset_phase_times()
+    s.advance_mov_window(100)
+    s.synchronize()
+    phases = {k: v[0] / 100 for k, v in s.phase_times().items()}
     if rank == 0:
         print(json.dumps({
             'metric': METRIC, 'value': pushes * world / t, 'unit': UNIT, 'n_gpus': world,
@@ -491,6 +497,7 @@ def run_lwfa(args, world, rank, local):
             'cell_updates_per_second': nx * ny * steps * world / t,
             'gpu_launches': s.launch_count() - l0,
             'field_energy_final': float(e.sum() + b.sum()),
+            'phase_ms_per_step': phases,
             'clocks': clk.summary(),
         }))
     s.close()

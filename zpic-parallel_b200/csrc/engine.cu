@@ -98,6 +98,7 @@ template < class T > static int dalloc( T ** p, size_t n ) {
 template < class T > static void dfree( T *& p ) { if ( p ) cudaFree( p ); p = nullptr; }
 
 static inline int roundup4( int n ) { return ( n + 3 ) & ~3; }
+constexpr int MAX_SPECIES = 64;     // species per simulation
 
 enum Phase { PH_PARTICLES = 0, PH_SORT, PH_CURRENT, PH_FIELDS, PH_OTHER, PH_N };
 
@@ -747,17 +748,13 @@ static int species_advance_mw( zpic_sim * s, int sp ) {
     TRY( ensure_plan( s ) );
     const float t = ( h->iter + 1 ) * h->dt;        // int * float, as in the reference
     if ( h->mw.needs_move( t ) ) {
-        std::vector<int> shifts( s->species.size(), 0 );
-        shifts[sp] = -1;
-        CK( cudaMemcpyAsync( s->shifts_d, shifts.data(), shifts.size() * sizeof( int ), cudaMemcpyHostToDevice, s->stream ) );
         TRY( species_kernel( s, sp, 1, 2, s->shifts_d ) );
         const unsigned gx = s->ntx * s->nxx, gy = s->nty * s->nxy;
         const unsigned range[4] = { gx - 1, gx - 1, 0, gy - 1 };
         InjRule r = inj_rule( s, h, range );
-        // host-side bound of the particle count (exact injection count)
-        std::vector<int> extra( h->ntiles, 0 );
-        injector( s, h ).count( range, extra.data() );
-        uint64_t add = 0; for ( int v : extra ) add += v;
+        // host-side upper bound of the particle count: at most a full
+        // column of cells is injected per move
+        const uint64_t add = h->dens.type == ZPIC_DENSITY_NONE ? 0 : (uint64_t) gy * h->ppc[0] * h->ppc[1];
         h->np_bound += add;
         if ( h->np_bound > h->max_part ) {
             // the bound is loose once particles leave; read the real count
@@ -851,7 +848,13 @@ int zpic_b200_sim_create( uint32_t ntx, uint32_t nty, uint32_t nxx, uint32_t nxy
     R.status = s->status;
     TRY( dalloc( &s->dscratch, 64 ) );
     CK( cudaMallocHost( (void **) &s->hscratch, 64 * sizeof( double ) ) );
-    TRY( dalloc( &s->shifts_d, 64 ) );
+    // cell shift of a moving-window step: -1 for whichever species the
+    // particle kernel is launched for (at most MAX_SPECIES per simulation)
+    TRY( dalloc( &s->shifts_d, MAX_SPECIES ) );
+    {
+        std::vector<int> neg( MAX_SPECIES, -1 );
+        CK( cudaMemcpy( s->shifts_d, neg.data(), MAX_SPECIES * sizeof( int ), cudaMemcpyHostToDevice ) );
+    }
     TRY( upload_run( s.get() ) );
     *out = s.release();
     return ZPIC_OK;
@@ -876,6 +879,7 @@ int zpic_b200_sim_add_species( zpic_sim * s, const zpic_species_desc * desc, int
     TRY( sim_select( s ) );
     if ( !desc ) return fail( ZPIC_E_INVALID, "null species description" );
     if ( desc->m_q == 0 ) return fail( ZPIC_E_INVALID, "Invalid m_q value, must be not 0" );          // species.cpp:1698
+    if ( s->species.size() >= (size_t) MAX_SPECIES ) return fail( ZPIC_E_INVALID, "too many species" );
     if ( desc->ppc[0] < 1 || desc->ppc[1] < 1 ) return fail( ZPIC_E_INVALID, "Invalid ppc value, must be >= 1 in all directions" );
     if ( desc->density.type < 0 || desc->density.type > 4 ) return fail( ZPIC_E_INVALID, "invalid density type" );
     if ( desc->udist.type < 0 || desc->udist.type > 3 ) return fail( ZPIC_E_INVALID, "invalid udist type" );
