@@ -362,6 +362,7 @@ def run_ensemble(args, world, rank, local):
     import torch
     import zpic_b200 as zb
     torch.cuda.set_device(local)
+    steps = args.steps if args.steps_given else 500
     specs = ensemble_specs(args.runs)
     specs = specs[rank::world]                  # runs shard across ranks, no exchange
     sims = []
@@ -395,10 +396,11 @@ def run_ensemble(args, world, rank, local):
         torch.cuda.synchronize()
         return max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, world)
 
+    chunks = batch.autotune(2) if args.autotune else None
     batch.advance(args.warmup)
     batch.synchronize()
     l0 = batch.launch_count()
-    tb = timed([bstream], lambda: batch.advance(args.steps))
+    tb = timed([bstream], lambda: batch.advance(steps))
     batch.synchronize()
     launches = batch.launch_count() - l0
     # plain: each run advanced on its own through its own CUDA graph, the runs
@@ -413,7 +415,7 @@ def run_ensemble(args, world, rank, local):
         for s, st in zip(sims, sstreams):
             if prev is not None:
                 st.wait_event(prev)
-            s.advance(args.steps)
+            s.advance(steps)
             prev = torch.cuda.Event()
             prev.record(st)
     tp = timed(sstreams, serial)
@@ -423,26 +425,27 @@ def run_ensemble(args, world, rank, local):
     # ... and all runs issued at once on their own streams
     def concurrent():
         for s in sims:
-            s.advance(args.steps)
+            s.advance(steps)
     tc = timed(sstreams, concurrent)
     for s in sims:
         s.synchronize()
     if rank == 0:
         print(json.dumps({
-            'metric': 'ensemble_run_steps_per_second', 'value': args.runs * args.steps / tb,
-            'unit': 'run-steps/s', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
-            'ms_per_step': tb / args.steps * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+            'metric': 'ensemble_run_steps_per_second', 'value': args.runs * steps / tb,
+            'unit': 'run-steps/s', 'n_gpus': world, 'steps': steps, 'warmup': args.warmup,
+            'ms_per_step': tb / steps * 1e3, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded)',
             'config': {'workload': 'Weibel ensemble, %d runs (seeded PCG64 draw of N, ppc, ufl, uth)' % args.runs,
                        'particles_per_rank': nparticles, 'runs_per_rank': len(sims)},
-            'plain': {'value': args.runs * args.steps / tp, 'unit': 'run-steps/s',
+            'plain': {'value': args.runs * steps / tp, 'unit': 'run-steps/s',
                       'how': 'each run through its own CUDA graph, runs one after another'},
-            'plain_concurrent': {'value': args.runs * args.steps / tc, 'unit': 'run-steps/s',
+            'plain_concurrent': {'value': args.runs * steps / tc, 'unit': 'run-steps/s',
                                  'how': 'each run through its own CUDA graph on its own stream, all issued at once'},
             'batched_over_plain': tp / tb,
             'batched_over_plain_concurrent': tc / tb,
-            'pushes_per_second': nparticles * world * args.steps / tb,
+            'pushes_per_second': nparticles * world * steps / tb,
             'gpu_launches': launches,
+            'ctas_per_tile': chunks if chunks is not None else 'automatic',
         }))
     batch.close()
     return 0
@@ -516,6 +519,7 @@ def main():
     ap.add_argument('--ref-cells', type=int, default=512, help='CPU sample size (cells per side)')
     ap.add_argument('--ref-steps', type=int, default=10)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--autotune', type=int, default=1, help='ensemble: autotune CTAs per tile first (1/0)')
     args = ap.parse_args()
     args.steps_given = any(a.startswith('--steps') for a in sys.argv[1:])
     args.warmup = max(3, args.warmup)

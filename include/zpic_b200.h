@@ -157,6 +157,14 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  *                         the additions; the fastest of the three)
  */
 int zpic_b200_sim_set_option( zpic_sim * sim, const char * key, double value );
+/* Autotuner (no reference counterpart): times `steps` steps for each
+ * candidate number of CTAs per tile (1, 2, 4, ... 64, at least 256 particles
+ * per CTA on average) and keeps the fastest ("chunks" option); *chosen gets
+ * it.  The trial steps are real Simulation::advance steps (each candidate
+ * runs 1 + steps of them); the choice changes no result beyond the FP32
+ * order in which per-CTA partial currents are added.  Not for moving-window
+ * simulations. */
+int zpic_b200_sim_autotune( zpic_sim * sim, int32_t steps, int32_t * chosen );
 /* Per-phase device time (ms) and launch counts accumulated while "profile" is on.
  * phases: 0 particle kernel, 1 sort, 2 current, 3 field solve, 4 other.  n <= 5. */
 int zpic_b200_sim_phase_times( zpic_sim * sim, double * ms, uint64_t * launches, int32_t n );
@@ -247,6 +255,8 @@ int zpic_b200_batch_create( zpic_sim * const * sims, int32_t n, zpic_batch ** ou
 int zpic_b200_batch_advance( zpic_batch * batch, int32_t nsteps );
 int zpic_b200_batch_synchronize( zpic_batch * batch );
 int zpic_b200_batch_destroy( zpic_batch * batch );
+/* The autotuner above for a batch: CTAs per tile for all of its runs. */
+int zpic_b200_batch_autotune( zpic_batch * batch, int32_t steps, int32_t * chosen );
 /* Kernel launches issued by batch steps since the batch was created. */
 int zpic_b200_batch_launch_count( zpic_batch * batch, uint64_t * count );
 /* The cudaStream_t a batch's steps run on (for external event timing). */

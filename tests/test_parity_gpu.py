@@ -118,7 +118,7 @@ def test_move_deposit_fp64_tile_current():
 
 
 def test_move_deposit_fixed_point_tile_current():
-    """Option "jacc" 2: 64-bit fixed-point tile current.  Positions bit-exact,
+    """Option "jacc" 2 (default): fixed-point tile current in two 32-bit words.  Positions bit-exact,
     current within the FP32 bar, and with one CTA per tile and two species
     (two FP32 additions per cell onto zero, which commute) the deposited
     current is the same bit for bit on every run."""
@@ -142,6 +142,25 @@ def test_move_deposit_fixed_point_tile_current():
     assert np.array_equal(runs[0], runs[1])
     with pytest.raises(zb.ZpicError):
         g.set_option('jacc', 3)
+
+
+def test_fixed_point_flush_dense_tiles():
+    """65,536 particles per tile in one CTA: the fixed-point tile current is
+    flushed to the raw current between groups of 16,384 particles; the
+    deposited current stays within the FP32 bar of the oracle's."""
+    geom = ((2, 2), (16, 16), (3.2, 3.2), 0.07)
+
+    def setup(s):
+        s.add_species(-1.0, (16, 16), udist=('thermal', (0.2, 0.2, 0.2), (0.05, 0, 0)))
+        return s
+    o, g = pair(setup, geom)
+    g.set_option('chunks', 1)
+    for s in (o, g):
+        s.current_zero()
+        s.species_move(0)
+    assert np.array_equal(o.particles(0)[2], g.particles(0)[2])
+    m = interior_mask(o)
+    assert rel_err(g.grid('J')[:, m], o.grid('J')[:, m]) <= J_TOL
 
 
 def test_tile_sort_multisets():

@@ -62,3 +62,30 @@ def test_grid_file_bytes_match_reference(writer, tmp_path, monkeypatch):
     assert [a['name'] for a in g['grid']['axis']] == ['x', 'y']
     assert abs(g['grid']['axis'][0]['max'] - 6.4) < 1e-6 and abs(g['grid']['axis'][1]['max'] - 3.2) < 1e-6
     assert np.array_equal(g['datasets']['Bz'], dense)
+    # the Python writer of the library writes the same bytes
+    import zpic_b200.zdf as pz
+    fn = pz.save_grid(dense, 'Bz', 'B_z', 'm_e c \\omega_n e^{-1}',
+                      [('x', 0.0, float(np.float32(6.4)), 'x', 'c/\\omega_n'),
+                       ('y', 0.0, float(np.float32(3.2)), 'y', 'c/\\omega_n')],
+                      3, 3 * 0.05, str(tmp_path / 'PY'))
+    assert open(fn, 'rb').read() == ref_b
+    fn = pz.save_grid(rho, 'species-charge', 'species \\rho', 'n_e',
+                      [('x', 0.0, float(np.float32(6.4)), 'x', 'c/\\omega_n'),
+                       ('y', 0.0, float(np.float32(3.2)), 'y', 'c/\\omega_n')],
+                      3, float(t32), str(tmp_path / 'PYC'), iter_name='ITERATION')
+    assert open(fn, 'rb').read() == ref_c
+
+
+def test_python_particle_file_layout(tmp_path):
+    """Particle files of the Python writer read back with the test reader."""
+    import zpic_b200.zdf as pz
+    from zdf_read import read
+    rng = np.random.default_rng(1)
+    q = [rng.random(100).astype(np.float32) for _ in range(5)]
+    fn = pz.save_particles(q, 'electrons', 'electrons', ['x', 'y', 'ux', 'uy', 'uz'],
+                           ['x', 'y', 'u_x', 'u_y', 'u_z'], ['c/\\omega_n'] * 2 + ['c'] * 3, 7, 0.49,
+                           str(tmp_path / 'PARTICLES'))
+    d = read(fn)
+    assert d['TYPE'] == 'particles' and d['particles']['np'] == 100 and d['iteration']['n'] == 7
+    for name, a in zip(['x', 'y', 'ux', 'uy', 'uz'], q):
+        assert np.array_equal(d['datasets'][name], a)

@@ -220,6 +220,7 @@ struct zpic_batch {
     Plan plan;
     cudaEvent_t ev = nullptr;
     uint64_t launches = 0;          // kernels launched by batch steps
+    int chunks = 0;                 // CTAs per tile chosen for the batch (0 = automatic)
 };
 
 static int sim_select( zpic_sim * s ) {
@@ -264,7 +265,7 @@ static int upload_run( zpic_sim * s ) {
 }
 
 // Build the work lists for a set of simulations (one sim, or a batch).
-static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims ) {
+static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunks_override = 0 ) {
     P.release();
     P.sims = sims;
     std::vector<RunDev> runs;
@@ -281,7 +282,8 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims ) {
     for ( auto * s : sims ) for ( auto * sp : s->species ) { (void) sp; total_tiles += s->ntx * s->nty; }
     // a batch chooses its CTAs per tile from all of its tiles; a single
     // simulation keeps the choice made for it
-    const int batch_chunks = sims.size() > 1 ? auto_chunks( std::max( 1, total_tiles ), 0 ) : 0;
+    const int batch_chunks = chunks_override > 0 ? chunks_override
+                           : sims.size() > 1 ? auto_chunks( std::max( 1, total_tiles ), 0 ) : 0;
     for ( size_t r = 0; r < sims.size(); r++ ) {
         zpic_sim * s = sims[r];
         runs.push_back( s->run );
@@ -781,6 +783,44 @@ static int species_advance_mw( zpic_sim * s, int sp ) {
     }
     h->iter++;
     return ZPIC_OK;
+}
+
+// ---- autotuning of CTAs per tile ----
+// Candidates: 1, 2, 4, ... 64 CTAs per tile, keeping at least 256 particles
+// per CTA on average, plus the automatic choice.  Each candidate runs one
+// untimed step (graph capture) and `steps` timed steps; the trial steps are
+// real steps of the simulation(s).  The physics does not depend on the
+// choice; only the order in which the per-CTA partial currents are added to
+// the raw current (FP32) does.
+static std::vector<int> chunk_candidates( uint64_t particles, uint64_t tiles, int automatic ) {
+    std::vector<int> c;
+    const double per_tile = tiles ? (double) particles / tiles : 0.0;
+    for ( int k = 1; k <= 64; k *= 2 )
+        if ( k == 1 || per_tile / k >= 256.0 ) c.push_back( k );
+    if ( std::find( c.begin(), c.end(), automatic ) == c.end() ) c.push_back( automatic );
+    return c;
+}
+
+template < class Advance >
+static int time_candidate( cudaStream_t st, int steps, Advance adv, float * ms ) {
+    cudaEvent_t e0, e1;
+    CK( cudaEventCreate( &e0 ) ); CK( cudaEventCreate( &e1 ) );
+    int rc = adv( 1 );
+    if ( rc == ZPIC_OK ) {
+        CK( cudaEventRecord( e0, st ) );
+        rc = adv( steps );
+        CK( cudaEventRecord( e1, st ) );
+        CK( cudaEventSynchronize( e1 ) );
+        CK( cudaEventElapsedTime( ms, e0, e1 ) );
+    }
+    cudaEventDestroy( e0 ); cudaEventDestroy( e1 );
+    return rc;
+}
+
+static uint64_t particles_of( zpic_sim * s ) {
+    uint64_t n = 0;
+    for ( auto * h : s->species ) n += h->np_bound;
+    return n;
 }
 
 // ---------------------------------------------------------------------------
@@ -1489,7 +1529,7 @@ int zpic_b200_batch_create( zpic_sim * const * sims, int32_t n, zpic_batch ** ou
     CK( cudaSetDevice( sims[0]->device ) );
     CK( cudaStreamCreateWithFlags( &b->stream, cudaStreamNonBlocking ) );
     CK( cudaEventCreateWithFlags( &b->ev, cudaEventDisableTiming ) );
-    TRY( plan_build( b->plan, b->sims ) );
+    TRY( plan_build( b->plan, b->sims, b->chunks ) );
     *out = b.release();
     return ZPIC_OK;
 }
@@ -1513,6 +1553,46 @@ int zpic_b200_batch_advance( zpic_batch * b, int32_t nsteps ) {
     b->launches += l;
     CK( cudaEventRecord( b->ev, b->stream ) );
     for ( auto * s : b->sims ) CK( cudaStreamWaitEvent( s->stream, b->ev, 0 ) );
+    return ZPIC_OK;
+}
+
+int zpic_b200_sim_autotune( zpic_sim * s, int32_t steps, int32_t * chosen ) {
+    TRY( sim_select( s ) );
+    if ( steps < 1 ) return fail( ZPIC_E_INVALID, "autotune needs at least one timed step" );
+    if ( s->species.empty() ) return fail( ZPIC_E_INVALID, "no species to tune for" );
+    if ( s->emf_mw.active ) return fail( ZPIC_E_INVALID, "autotune runs Simulation::advance steps; not for moving-window runs" );
+    uint64_t ntiles = 0; for ( auto * h : s->species ) ntiles += h->ntiles;
+    const int automatic = auto_chunks( (int) ntiles, 0 );
+    int best = automatic; float best_ms = -1;
+    for ( int c : chunk_candidates( particles_of( s ), ntiles, automatic ) ) {
+        TRY( zpic_b200_sim_set_option( s, "chunks", c ) );
+        float ms = 0;
+        TRY( time_candidate( s->stream, steps, [&]( int n ) { return zpic_b200_sim_advance( s, n ); }, &ms ) );
+        if ( best_ms < 0 || ms < best_ms ) { best_ms = ms; best = c; }
+    }
+    TRY( zpic_b200_sim_set_option( s, "chunks", best ) );
+    if ( chosen ) *chosen = best;
+    return ZPIC_OK;
+}
+
+int zpic_b200_batch_autotune( zpic_batch * b, int32_t steps, int32_t * chosen ) {
+    if ( !b ) return fail( ZPIC_E_INVALID, "null batch" );
+    if ( steps < 1 ) return fail( ZPIC_E_INVALID, "autotune needs at least one timed step" );
+    CK( cudaSetDevice( b->sims[0]->device ) );
+    uint64_t ntiles = 0, np = 0;
+    for ( auto * s : b->sims ) { np += particles_of( s ); for ( auto * h : s->species ) ntiles += h->ntiles; }
+    const int automatic = auto_chunks( (int) std::min<uint64_t>( ntiles, 1u << 30 ), 0 );
+    int best = automatic; float best_ms = -1;
+    for ( int c : chunk_candidates( np, ntiles, automatic ) ) {
+        b->chunks = c;
+        TRY( plan_build( b->plan, b->sims, c ) );
+        float ms = 0;
+        TRY( time_candidate( b->stream, steps, [&]( int n ) { return zpic_b200_batch_advance( b, n ); }, &ms ) );
+        if ( best_ms < 0 || ms < best_ms ) { best_ms = ms; best = c; }
+    }
+    b->chunks = best;
+    TRY( plan_build( b->plan, b->sims, best ) );
+    if ( chosen ) *chosen = best;
     return ZPIC_OK;
 }
 

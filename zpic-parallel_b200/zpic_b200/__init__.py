@@ -40,6 +40,7 @@ EXPORTS = [
     'zpic_b200_sim_phase_times', 'zpic_b200_sim_reset_phase_times', 'zpic_b200_sim_launch_count',
     'zpic_b200_sim_stream',
     'zpic_b200_batch_stream', 'zpic_b200_batch_launch_count',
+    'zpic_b200_sim_autotune', 'zpic_b200_batch_autotune',
     'zpic_b200_emf_set_bc', 'zpic_b200_emf_advance', 'zpic_b200_emf_energy', 'zpic_b200_laser_add',
     'zpic_b200_current_set_bc', 'zpic_b200_current_set_filter', 'zpic_b200_current_zero',
     'zpic_b200_current_advance',
@@ -117,6 +118,8 @@ def lib():
             'zpic_b200_sim_stream': (I, [P, ctypes.POINTER(P)]),
             'zpic_b200_batch_stream': (I, [P, ctypes.POINTER(P)]),
             'zpic_b200_batch_launch_count': (I, [P, ctypes.POINTER(ctypes.c_uint64)]),
+            'zpic_b200_sim_autotune': (I, [P, I, IP]),
+            'zpic_b200_batch_autotune': (I, [P, I, IP]),
             'zpic_b200_emf_set_bc': (I, [P, IP]),
             'zpic_b200_emf_advance': (I, [P, I]),
             'zpic_b200_emf_energy': (I, [P, DP, DP]),
@@ -286,6 +289,12 @@ class Simulation:
 
     def set_option(self, key, value):
         _check(lib().zpic_b200_sim_set_option(self.h, key.encode(), float(value)))
+
+    def autotune(self, steps=3):
+        """Pick the CTAs per tile by timing real steps; returns the choice."""
+        v = ctypes.c_int()
+        _check(lib().zpic_b200_sim_autotune(self.h, int(steps), ctypes.byref(v)))
+        return v.value
 
     # ---- stepping ----
     def advance(self, n=1):
@@ -462,6 +471,12 @@ class Batch:
     def launch_count(self):
         v = ctypes.c_uint64()
         _check(lib().zpic_b200_batch_launch_count(self.h, ctypes.byref(v)))
+        return v.value
+
+    def autotune(self, steps=3):
+        """Pick the CTAs per tile for all runs by timing real batch steps."""
+        v = ctypes.c_int()
+        _check(lib().zpic_b200_batch_autotune(self.h, int(steps), ctypes.byref(v)))
         return v.value
 
     def stream_handle(self):
