@@ -476,7 +476,9 @@ def run_lwfa(args, world, rank, local):
     l0, n0 = s.launch_count(), s.nmove()
     with ClockSampler(local) as clk:
         ev0.record(stream)
+        h0 = time.perf_counter()
         s.advance_mov_window(steps)
+        host_s = time.perf_counter() - h0       # time the host takes to issue the steps
         ev1.record(stream)
         ev1.synchronize()
     t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
@@ -501,15 +503,78 @@ def run_lwfa(args, world, rank, local):
             'gpu_launches': s.launch_count() - l0,
             'field_energy_final': float(e.sum() + b.sum()),
             'phase_ms_per_step': phases,
+            'host_issue_ms_per_step': host_s / steps * 1e3,
             'clocks': clk.summary(),
         }))
     s.close()
     return 0
 
 
+def reference_cuda(ppc, ntiles, timeout=900):
+    """The reference's own CUDA build (oracle/_ref/cuda/zpic, sm_100a) on its
+    Weibel test: 32x32 tiles, two species, 500 steps.  Returns its printed
+    GPart/s (host-timed around the step loop by the reference) or None."""
+    exe = os.path.join(ROOT, 'oracle', '_ref', 'cuda', 'zpic')
+    if not os.path.exists(exe):
+        return None, 'reference CUDA build oracle/_ref/cuda/zpic missing'
+    r = subprocess.run([exe, '-s', '-t', 'weibel', '-p', '%d,%d,%d,%d' % (ppc, ppc, ntiles, ntiles)],
+                       capture_output=True, text=True, timeout=timeout)
+    m = re.search(r'Performance:\s*([0-9.eE+-]+)\s*GPart/s', r.stdout)
+    if r.returncode != 0 or not m:
+        return None, 'reference run failed (rc %d): %s' % (r.returncode, (r.stdout + r.stderr)[-300:])
+    return float(m.group(1)) * 1e9, r.stdout[-400:]
+
+
+def run_weibel(args, world, rank, local):
+    """Weibel instability at scale, the reference CUDA driver's own test
+    (cuda/em2d/main.cpp:613-692): 32x32 tiles, ntiles x ntiles tiles, box
+    0.1 per cell, dt 0.07, electrons and positrons 8x8 ppc ThermalCorr uth
+    0.1, uz +-0.6, 500 steps.  Timed on the device; with --reference-gpu the
+    reference's own CUDA build runs the same test on the same GPU."""
+    import torch
+    import zpic_b200 as zb
+    torch.cuda.set_device(local)
+    nt, ppc = args.weibel_tiles, 8
+    steps = args.steps if args.steps_given else 500
+    s = zb.Simulation((nt, nt), (32, 32), (nt * 32 * 0.1, nt * 32 * 0.1), 0.07, device=local)
+    s.add_species(-1.0, (ppc, ppc), udist=('thermalcorr', (0.1, 0.1, 0.1), (0, 0, 0.6)), name='electrons')
+    s.add_species(1.0, (ppc, ppc), udist=('thermalcorr', (0.1, 0.1, 0.1), (0, 0, -0.6)), name='positrons')
+    npart = s.np_total(0) + s.np_total(1)
+    stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    n0 = s.nmove()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        s.advance(steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
+    pushes = s.nmove() - n0
+    s.close()
+    ref = None
+    if args.reference_gpu and rank == 0 and world == 1:
+        rate, info = reference_cuda(ppc, nt)
+        ref = {'value': rate, 'unit': UNIT, 'kind': 'reference CUDA build (cuda/em2d, sm_100a), same GPU',
+               'timing': 'host timer around its 500-step loop', 'info': info}
+    if rank == 0:
+        print(json.dumps({
+            'metric': METRIC, 'value': pushes * world / t, 'unit': UNIT, 'n_gpus': world,
+            'steps': steps, 'warmup': 0, 'ms_per_step': t / steps * 1e3, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded)',
+            'config': {'workload': 'Weibel %dx%d cells, 32x32 tiles, 2 species x 8x8 ppc, %d steps'
+                                   % (nt * 32, nt * 32, steps), 'particles': npart},
+            'reference_gpu': ref, 'clocks': clk.summary(),
+        }))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--workload', default='plasma', choices=['plasma', 'ensemble', 'lwfa'])
+    ap.add_argument('--workload', default='plasma', choices=['plasma', 'ensemble', 'lwfa', 'weibel'])
+    ap.add_argument('--weibel-tiles', type=int, default=64, help='weibel: tiles per side (32x32 cells each)')
+    ap.add_argument('--reference-gpu', type=int, default=1, help='weibel: also run the reference CUDA build')
     ap.add_argument('--runs', type=int, default=256, help='ensemble runs (--workload ensemble)')
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=20)
@@ -531,6 +596,8 @@ def main():
             rc = run_ensemble(args, world, rank, local)
         elif args.workload == 'lwfa':
             rc = run_lwfa(args, world, rank, local)
+        elif args.workload == 'weibel':
+            rc = run_weibel(args, world, rank, local)
         else:
             rc = run_gpu(args, world, rank, local)
     finally:

@@ -198,6 +198,9 @@ int zpic_b200_species_set_push_type( zpic_sim * sim, int32_t sp, int32_t type );
 int zpic_b200_species_energy( zpic_sim * sim, int32_t sp, double * energy );   /* Species::get_energy (species.h:365) */
 int zpic_b200_species_nmove( zpic_sim * sim, int32_t sp, uint64_t * nmove );   /* Species::get_nmove */
 int zpic_b200_species_np_total( zpic_sim * sim, int32_t sp, uint64_t * np );   /* Species::np_total */
+/* Times the tile sort had to rebuild the slot layout of this species (a full
+ * copy of its particles through the second buffer); no reference counterpart. */
+int zpic_b200_species_repacks( zpic_sim * sim, int32_t sp, uint64_t * repacks );
 int zpic_b200_species_np_max_tile( zpic_sim * sim, int32_t sp, uint32_t * np );/* Species::np_max_tile */
 /* Tile information in the reference's packed layout: offset[t] = sum of np before t (particles.h:94-97) */
 int zpic_b200_species_get_tiles( zpic_sim * sim, int32_t sp, int32_t * np, int32_t * offset );

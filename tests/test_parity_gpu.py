@@ -330,3 +330,43 @@ def test_diagnostics_charge_and_phasespace():
     # a large phase space goes through global atomics instead of a shared copy
     big = s.phasespace(0, 'x', (0.0, 12.8), 256, 'uz', (-1.5, 1.5), 256)
     assert close(big, o.phasespace(0, 0, (0.0, 12.8), 256, 4, (-1.5, 1.5), 256), 1e-5)
+
+
+def test_weibel_growth_rate():
+    """Weibel growth rate from the magnetic energy history: the exponential
+    rate fitted over the linear phase agrees with the oracle's within 1e-3."""
+    o, g = pair(weibel)
+    eb_o, eb_g = [], []
+    for _ in range(250):
+        o.advance(1)
+        g.advance(1)
+        eb_o.append(o.emf_energy()[1].sum())
+        eb_g.append(g.emf_energy()[1].sum())
+    eb_o, eb_g = np.log(np.array(eb_o)), np.log(np.array(eb_g))
+    # growth phase: steps 30 to 230 (log E_B rises by ~7 e-folds, with the
+    # plasma oscillation on top, the same in both histories)
+    sel = np.arange(30, 230)
+    t = (sel + 1) * WEIBEL[3]
+    rate_o = np.polyfit(t, eb_o[sel], 1)[0]
+    rate_g = np.polyfit(t, eb_g[sel], 1)[0]
+    assert rate_o > 0
+    assert abs(rate_g - rate_o) <= 1e-3 * rate_o
+
+
+def test_moving_window_graph_replay():
+    """Moving-window steps replayed from CUDA graphs (one per pattern of window
+    moves) against the same steps issued one by one: same particle counts per
+    tile, energies equal up to FP32 summation order."""
+    a = lwfa_small(zb.Simulation(*LWFA))
+    b = lwfa_small(zb.Simulation(*LWFA))
+    b.set_option('graph', 0)
+    for n in range(1, 81):
+        a.advance_mov_window(1 if n < 40 else 2)
+        b.advance_mov_window(1 if n < 40 else 2)
+        if a.iter() >= 80:
+            break
+    assert a.iter() == b.iter()
+    assert np.array_equal(a.tiles(0)[0], b.tiles(0)[0])
+    ea, eb = a.emf_energy(), b.emf_energy()
+    assert rel_err(a.species_energy(0), b.species_energy(0)) <= 1e-5
+    assert rel_err(ea[0].sum() + ea[1].sum(), eb[0].sum() + eb[1].sum()) <= 1e-5

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -23,15 +24,13 @@
 
 namespace zb {
 struct TileItem { int run; int tile; };
-struct InjRule {
-    int type; int diry; float a, b; float cx, cy, r2; float dxx, dxy; int ppcx, ppcy; int range[4]; int tx_limit;
-};
 size_t particle_smem_bytes( int tile_vol, int jacc );
 size_t yee_smem_bytes( int tile_vol );
 cudaError_t launch_particles( cudaStream_t, int, int, int, const Item *, int, const SpDev *, const RunDev *, const int *,
                               int, int, int );
 cudaError_t launch_sort( cudaStream_t, const Item *, int, const SpDev *, const int *, int, const RunDev *, int );
 cudaError_t launch_inject( cudaStream_t, int, int, const SpDev *, const RunDev *, const InjRule &, int );
+cudaError_t launch_inj_dyn( cudaStream_t, float *, unsigned *, int, float, float, float, double );
 cudaError_t launch_pack( cudaStream_t, int, int, const SpDev *, const int *, int2 *, float2 *, float * );
 cudaError_t launch_unpack( cudaStream_t, int, int, const SpDev *, const int *, const int2 *, const float2 *, const float * );
 cudaError_t launch_gather( cudaStream_t, int, int, const SpDev *, const RunDev *, const int *, int, float, float, int, float * );
@@ -39,9 +38,9 @@ cudaError_t launch_dep_charge( cudaStream_t, int, int, const SpDev *, const RunD
 cudaError_t launch_phasespace( cudaStream_t, int, int, const SpDev *, const RunDev *, PhaSpec, float * );
 cudaError_t launch_energy_sum( cudaStream_t, const SpDev *, int, int, double * );
 cudaError_t launch_np_stats( cudaStream_t, const SpDev *, int, unsigned long long * );
-cudaError_t launch_current_gc( cudaStream_t, const TileItem *, int, const RunDev * );
-cudaError_t launch_emf_gc( cudaStream_t, const TileItem *, int, const RunDev *, int );
-cudaError_t launch_cur_gc( cudaStream_t, const TileItem *, int, const RunDev *, int );
+cudaError_t launch_current_gc( cudaStream_t, const TileItem *, int, const RunDev *, int );
+cudaError_t launch_emf_gc( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
+cudaError_t launch_cur_gc( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
 cudaError_t launch_yee( cudaStream_t, const TileItem *, int, const RunDev *, int, int, int, int );
 cudaError_t launch_emf_bc( cudaStream_t, const RunDev *, int, int, int );
 cudaError_t launch_cur_bc( cudaStream_t, const RunDev *, int, int, int );
@@ -76,6 +75,12 @@ void set_last_error( const std::string & msg ) { g_err = msg; }
     } while ( 0 )
 
 #define TRY( call ) do { int r_ = ( call ); if ( r_ != ZPIC_OK ) return r_; } while ( 0 )
+
+// Device work of the step paths goes through DEV: when a moving-window step
+// is replayed from a CUDA graph, the same host code runs once more for its
+// bookkeeping with g_dry set, and issues nothing.
+static thread_local bool g_dry = false;
+#define DEV( call ) do { if ( !g_dry ) CK( call ); } while ( 0 )
 
 // ---------------------------------------------------------------------------
 // helpers
@@ -122,6 +127,8 @@ struct HSpecies {
     bool sort_pending = false;
     bool counters_dirty = false;
     int energy_items = 0;      // per-item energy partials written by the last push
+    float * inj_dyn = nullptr;         // window-dependent injection parameters (device)
+    unsigned * mw_nmove_d = nullptr;   // device copy of the window's move count
 
     void free_all() {
         PartArrays * arrs[3] = { &d.A, &d.B, &d.S };
@@ -129,7 +136,7 @@ struct HSpecies {
         dfree( d.np ); dfree( d.off ); dfree( d.cap ); dfree( d.nidx ); dfree( d.idx );
         dfree( d.aux ); dfree( d.aux2 ); dfree( d.in_cnt ); dfree( d.stage_off ); dfree( d.stage_cnt );
         dfree( d.new_off ); dfree( d.new_cap ); dfree( d.new_np ); dfree( d.extra ); dfree( d.mode );
-        dfree( d.energy ); dfree( d.nmove );
+        dfree( d.energy ); dfree( d.nmove ); dfree( inj_dyn ); dfree( mw_nmove_d );
     }
 };
 
@@ -158,15 +165,20 @@ struct Plan {
     std::vector<int> sp_k1_off, sp_k1_n, sp_sort_off, sp_sort_n;
     TileItem * tile_items_d = nullptr; int n_tiles = 0;
     int max_tile_vol = 0;
+    int max_cells = 0, max_guard = 0;   // cells and guard cells of the largest tile
     int jacc = 0;                   // tile current accumulation (option "jacc")
     int tile_n = 0;                 // n when every run has n x n tiles with a specialised kernel
     bool needs_bc_or_filter = false;
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
+    // moving-window steps, one graph per pattern of window moves
+    std::map<unsigned, std::pair<cudaGraphExec_t, int>> mw_graphs;
     bool built = false;
 
     void release() {
         if ( graph ) { cudaGraphExecDestroy( graph ); graph = nullptr; }
+        for ( auto & g : mw_graphs ) cudaGraphExecDestroy( g.second.first );
+        mw_graphs.clear();
         dfree( runs_d ); dfree( sps_d ); dfree( k1_items_d[0] ); dfree( k1_items_d[1] );
         dfree( sort_items_d ); dfree( splist_d ); dfree( tile_items_d ); dfree( spk1_d );
         built = false;
@@ -275,6 +287,7 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
     P.sps_h.clear(); P.sp_sim.clear(); P.sp_local.clear();
     P.sp_k1_off.clear(); P.sp_k1_n.clear(); P.sp_sort_off.clear(); P.sp_sort_n.clear();
     P.max_tile_vol = 0;
+    P.max_cells = 0; P.max_guard = 0;
     P.jacc = -1;
     P.tile_n = -1;
     P.needs_bc_or_filter = false;
@@ -288,6 +301,8 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
         zpic_sim * s = sims[r];
         runs.push_back( s->run );
         P.max_tile_vol = std::max( P.max_tile_vol, s->run.tile_vol );
+        P.max_cells = std::max( P.max_cells, s->run.extx * s->run.exty );
+        P.max_guard = std::max( P.max_guard, s->run.extx * s->run.exty - s->run.nxx * s->run.nxy );
         // one accumulation mode per plan: the runs' own when they agree
         P.jacc = ( P.jacc < 0 || P.jacc == s->jacc ) ? s->jacc : 2;
         const int tn = ( s->nxx == 16 && s->nxy == 16 ) ? 16 : 0;
@@ -388,7 +403,7 @@ static int run_particles( Plan & P, cudaStream_t st, int push, int move, const i
     for ( int p = 0; p < 2; p++ ) {
         if ( P.n_k1[p] == 0 ) continue;
         PhaseScope ps( prof_sim( P ), st, PH_PARTICLES, 1 );
-        CK( launch_particles( st, push ? p + 1 : 0, move, 1, P.k1_items_d[p], P.n_k1[p], P.sps_d, P.runs_d, shifts, P.max_tile_vol,
+        DEV( launch_particles( st, push ? p + 1 : 0, move, 1, P.k1_items_d[p], P.n_k1[p], P.sps_d, P.runs_d, shifts, P.max_tile_vol,
                               P.jacc, P.tile_n ) );
     }
     return ZPIC_OK;
@@ -397,7 +412,7 @@ static int run_particles( Plan & P, cudaStream_t st, int push, int move, const i
 static int run_sort( Plan & P, cudaStream_t st, int use_extra ) {
     if ( P.n_sp == 0 ) return ZPIC_OK;
     PhaseScope ps( prof_sim( P ), st, PH_SORT, 3 );
-    CK( launch_sort( st, P.sort_items_d, P.n_sort, P.sps_d, P.splist_d, P.n_sp, P.runs_d, use_extra ) );
+    DEV( launch_sort( st, P.sort_items_d, P.n_sort, P.sps_d, P.splist_d, P.n_sp, P.runs_d, use_extra ) );
     return ZPIC_OK;
 }
 
@@ -405,18 +420,18 @@ static int run_sort( Plan & P, cudaStream_t st, int use_extra ) {
 static int run_current( Plan & P, cudaStream_t st ) {
     {
         PhaseScope ps( prof_sim( P ), st, PH_CURRENT, 1 );
-        CK( launch_current_gc( st, P.tile_items_d, P.n_tiles, P.runs_d ) );
+        DEV( launch_current_gc( st, P.tile_items_d, P.n_tiles, P.runs_d, P.max_cells ) );
     }
     if ( !P.needs_bc_or_filter ) return ZPIC_OK;
     for ( size_t r = 0; r < P.sims.size(); r++ ) {
         zpic_sim * s = P.sims[r];
         if ( s->cur_bc[0] > 1 || s->cur_bc[1] > 1 ) {
             PhaseScope ps( prof_sim( P ), st, PH_CURRENT, 1 );
-            CK( launch_cur_bc( st, P.runs_d, (int) r, 0, 2 * s->nty * s->run.exty ) );
+            DEV( launch_cur_bc( st, P.runs_d, (int) r, 0, 2 * s->nty * s->run.exty ) );
         }
         if ( s->cur_bc[2] > 1 || s->cur_bc[3] > 1 ) {
             PhaseScope ps( prof_sim( P ), st, PH_CURRENT, 1 );
-            CK( launch_cur_bc( st, P.runs_d, (int) r, 1, 2 * s->ntx * s->run.extx ) );
+            DEV( launch_cur_bc( st, P.runs_d, (int) r, 1, 2 * s->ntx * s->run.extx ) );
         }
     }
     // filters (filter.h:22-86): run-specific, launched over all tiles of the plan only when uniform
@@ -431,8 +446,8 @@ static int run_current( Plan & P, cudaStream_t st ) {
         const TileItem * items = P.tile_items_d + first;
         auto pass = [&]( float a, float b, float c ) -> int {
             PhaseScope ps( prof_sim( P ), st, PH_CURRENT, 2 );
-            CK( launch_kernel3( st, items, nt, P.runs_d, 2, s->fdir, a, b, c, P.max_tile_vol ) );
-            CK( launch_cur_gc( st, items, nt, P.runs_d, s->fdir ? 2 : 1 ) );
+            DEV( launch_kernel3( st, items, nt, P.runs_d, 2, s->fdir, a, b, c, P.max_tile_vol ) );
+            DEV( launch_cur_gc( st, items, nt, P.runs_d, s->fdir ? 2 : 1, P.max_guard ) );
             return ZPIC_OK;
         };
         for ( unsigned i = 0; i < order; i++ ) TRY( pass( 0.25f, 0.5f, 0.25f ) );
@@ -450,19 +465,19 @@ static int run_current( Plan & P, cudaStream_t st ) {
 static int run_fields( Plan & P, cudaStream_t st, int with_j, int j_raw, int clear_jdep ) {
     {
         PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 2 );
-        CK( launch_yee( st, P.tile_items_d, P.n_tiles, P.runs_d, with_j, j_raw, clear_jdep, P.max_tile_vol ) );
-        CK( launch_emf_gc( st, P.tile_items_d, P.n_tiles, P.runs_d, 3 ) );
+        DEV( launch_yee( st, P.tile_items_d, P.n_tiles, P.runs_d, with_j, j_raw, clear_jdep, P.max_tile_vol ) );
+        DEV( launch_emf_gc( st, P.tile_items_d, P.n_tiles, P.runs_d, 3, P.max_guard ) );
     }
     if ( !P.needs_bc_or_filter ) return ZPIC_OK;
     for ( size_t r = 0; r < P.sims.size(); r++ ) {
         zpic_sim * s = P.sims[r];
         if ( s->emf_bc[0] > 1 || s->emf_bc[1] > 1 ) {
             PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 1 );
-            CK( launch_emf_bc( st, P.runs_d, (int) r, 0, 2 * s->nty * s->run.exty ) );
+            DEV( launch_emf_bc( st, P.runs_d, (int) r, 0, 2 * s->nty * s->run.exty ) );
         }
         if ( s->emf_bc[2] > 1 || s->emf_bc[3] > 1 ) {
             PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 1 );
-            CK( launch_emf_bc( st, P.runs_d, (int) r, 1, 2 * s->ntx * s->run.extx ) );
+            DEV( launch_emf_bc( st, P.runs_d, (int) r, 1, 2 * s->ntx * s->run.extx ) );
         }
     }
     return ZPIC_OK;
@@ -474,8 +489,8 @@ static int run_shift( Plan & P, cudaStream_t st, int r ) {
     for ( int q = 0; q < r; q++ ) first += P.sims[q]->ntx * P.sims[q]->nty;
     const int nt = P.sims[r]->ntx * P.sims[r]->nty;
     PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 2 );
-    CK( launch_shift_left( st, P.tile_items_d + first, nt, P.runs_d, P.max_tile_vol ) );
-    CK( launch_emf_gc( st, P.tile_items_d + first, nt, P.runs_d, 1 ) );
+    DEV( launch_shift_left( st, P.tile_items_d + first, nt, P.runs_d, P.max_tile_vol ) );
+    DEV( launch_emf_gc( st, P.tile_items_d + first, nt, P.runs_d, 1, P.max_guard ) );
     return ZPIC_OK;
 }
 
@@ -486,7 +501,7 @@ static int ensure_plan( zpic_sim * s ) {
 
 static int ensure_jdep_clean( zpic_sim * s, cudaStream_t st ) {
     if ( !s->jdep_clean ) {
-        CK( cudaMemsetAsync( s->run.Jdep, 0, s->grid_floats() * sizeof( float ), st ) );
+        DEV( cudaMemsetAsync( s->run.Jdep, 0, s->grid_floats() * sizeof( float ), st ) );
         s->jdep_clean = true;
     }
     return ZPIC_OK;
@@ -639,8 +654,10 @@ static int species_alloc( zpic_sim * s, HSpecies * sp, uint64_t max_part ) {
     TRY( dalloc( &d.in_cnt, nt ) ); TRY( dalloc( &d.stage_off, nt ) ); TRY( dalloc( &d.stage_cnt, nt ) );
     TRY( dalloc( &d.new_off, nt ) ); TRY( dalloc( &d.new_cap, nt ) ); TRY( dalloc( &d.new_np, nt ) );
     TRY( dalloc( &d.extra, nt ) ); TRY( dalloc( &d.mode, 1 ) );
-    TRY( dalloc( &d.nmove, 1 ) );
-    CK( cudaMemset( d.nmove, 0, sizeof( unsigned long long ) ) );
+    TRY( dalloc( &sp->inj_dyn, 4 ) ); TRY( dalloc( &sp->mw_nmove_d, 1 ) );
+    CK( cudaMemset( sp->mw_nmove_d, 0, sizeof( unsigned ) ) );
+    TRY( dalloc( &d.nmove, 2 ) );
+    CK( cudaMemset( d.nmove, 0, 2 * sizeof( unsigned long long ) ) );
     CK( cudaMemset( d.extra, 0, nt * sizeof( int ) ) );
     CK( cudaMemset( d.mode, 0, sizeof( int ) ) );
     return ZPIC_OK;
@@ -706,13 +723,13 @@ static int species_kernel( zpic_sim * s, int sp, int push, int move, const int *
     TRY( ensure_plan( s ) );
     HSpecies * h = s->species[sp];
     if ( h->counters_dirty && move ) {
-        CK( cudaMemsetAsync( h->d.in_cnt, 0, h->ntiles * sizeof( int ), s->stream ) );
-        CK( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
+        DEV( cudaMemsetAsync( h->d.in_cnt, 0, h->ntiles * sizeof( int ), s->stream ) );
+        DEV( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
     }
     Plan & P = s->plan;
     {
         PhaseScope ps( s, s->stream, PH_PARTICLES, 1 );
-        CK( launch_particles( s->stream, push ? 1 + h->push_type : 0, move, move ? 1 : 0,
+        DEV( launch_particles( s->stream, push ? 1 + h->push_type : 0, move, move ? 1 : 0,
                               P.spk1_d + P.sp_k1_off[sp], P.sp_k1_n[sp], P.sps_d, P.runs_d, shifts, P.max_tile_vol,
                               P.jacc, P.tile_n ) );
     }
@@ -728,15 +745,15 @@ static int species_sort( zpic_sim * s, int sp, int use_extra ) {
     Plan & P = s->plan;
     if ( !h->sort_pending ) {
         // leaver lists are stale: detect them now (bnd_check, particles.cpp:212-303)
-        CK( cudaMemsetAsync( h->d.in_cnt, 0, h->ntiles * sizeof( int ), s->stream ) );
-        CK( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
+        DEV( cudaMemsetAsync( h->d.in_cnt, 0, h->ntiles * sizeof( int ), s->stream ) );
+        DEV( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
         PhaseScope ps( s, s->stream, PH_SORT, 1 );
-        CK( launch_particles( s->stream, 0, 0, 1, P.spk1_d + P.sp_k1_off[sp], P.sp_k1_n[sp], P.sps_d, P.runs_d,
+        DEV( launch_particles( s->stream, 0, 0, 1, P.spk1_d + P.sp_k1_off[sp], P.sp_k1_n[sp], P.sps_d, P.runs_d,
                               nullptr, P.max_tile_vol, 0, 0 ) );
     }
     {
         PhaseScope ps( s, s->stream, PH_SORT, 3 );
-        CK( launch_sort( s->stream, P.sort_items_d + P.sp_sort_off[sp], P.sp_sort_n[sp], P.sps_d,
+        DEV( launch_sort( s->stream, P.sort_items_d + P.sp_sort_off[sp], P.sp_sort_n[sp], P.sps_d,
                          P.splist_d + sp, 1, P.runs_d, use_extra ) );
     }
     h->sort_pending = false;
@@ -761,19 +778,23 @@ static int species_advance_mw( zpic_sim * s, int sp ) {
         if ( h->np_bound > h->max_part ) {
             // the bound is loose once particles leave; read the real count
             unsigned long long st2[2];
-            CK( launch_np_stats( s->stream, s->plan.sps_d, sp, (unsigned long long *) s->dscratch ) );
+            DEV( launch_np_stats( s->stream, s->plan.sps_d, sp, (unsigned long long *) s->dscratch ) );
             CK( cudaMemcpyAsync( st2, s->dscratch, sizeof( st2 ), cudaMemcpyDeviceToHost, s->stream ) );
             CK( cudaStreamSynchronize( s->stream ) );
             h->np_bound = st2[0] + add;
             if ( h->np_bound > h->max_part ) return fail( ZPIC_E_NOMEM, "particle buffer too small for the moving-window injection" );
         }
         if ( h->dens.type != ZPIC_DENSITY_NONE ) {
-            CK( launch_inject( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, r, 1 ) );
-            s->launches++;
+            // the window-dependent rule parameters come from the device's move count
+            DEV( launch_inj_dyn( s->stream, h->inj_dyn, h->mw_nmove_d, h->dens.type, h->dens.a, h->dens.b,
+                                 h->dx[0], h->mw.dx ) );
+            r.dyn = h->inj_dyn;
+            DEV( launch_inject( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, r, 1 ) );
+            s->launches += 2;
         }
         TRY( species_sort( s, sp, h->dens.type != ZPIC_DENSITY_NONE ) );
         if ( h->dens.type != ZPIC_DENSITY_NONE ) {
-            CK( launch_inject( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, r, 0 ) );
+            DEV( launch_inject( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, r, 0 ) );
             s->launches++;
         }
         h->mw.advance();
@@ -1044,25 +1065,76 @@ int zpic_b200_sim_advance( zpic_sim * s, int32_t nsteps ) {
     return ZPIC_OK;
 }
 
+// One Simulation::advance_mov_window step (simulation.h:113-130): species,
+// current, fields and the window shift, issued on the simulation's stream.
+static int mw_step( zpic_sim * s ) {
+    TRY( ensure_jdep_clean( s, s->stream ) );
+    s->j_final = false;
+    for ( size_t k = 0; k < s->species.size(); k++ ) TRY( species_advance_mw( s, (int) k ) );
+    TRY( run_current( s->plan, s->stream ) );
+    s->cur_iter++;
+    if ( s->cur_mw.needs_move( s->cur_iter * s->dt ) ) s->cur_mw.advance();
+    TRY( run_fields( s->plan, s->stream, 1, 0, 1 ) );
+    s->jdep_clean = true;
+    s->j_final = true;
+    s->emf_iter++;
+    if ( s->emf_mw.active && s->emf_mw.needs_move( s->emf_iter * s->dt ) ) {
+        TRY( run_shift( s->plan, s->stream, 0 ) );
+        s->emf_mw.advance();
+    }
+    s->iter++;
+    return ZPIC_OK;
+}
+
+// Moving-window steps replay CUDA graphs: the device work of a step depends
+// only on which windows move in it (the window-dependent injection
+// parameters are computed on the device), so one graph per pattern of moves
+// is captured the first time it occurs.  Replays run the step's host code
+// once more with device work suppressed, for its bookkeeping.  Steps in which
+// a species' particle bound must be checked against the device (a host
+// synchronisation) run without a graph.
 int zpic_b200_sim_advance_mov_window( zpic_sim * s, int32_t nsteps ) {
     TRY( sim_select( s ) );
     TRY( ensure_plan( s ) );
     for ( int n = 0; n < nsteps; n++ ) {
-        TRY( ensure_jdep_clean( s, s->stream ) );
-        s->j_final = false;
-        for ( size_t k = 0; k < s->species.size(); k++ ) TRY( species_advance_mw( s, (int) k ) );
-        TRY( run_current( s->plan, s->stream ) );
-        s->cur_iter++;
-        if ( s->cur_mw.needs_move( s->cur_iter * s->dt ) ) s->cur_mw.advance();
-        TRY( run_fields( s->plan, s->stream, 1, 0, 1 ) );
-        s->jdep_clean = true;
-        s->j_final = true;
-        s->emf_iter++;
-        if ( s->emf_mw.active && s->emf_mw.needs_move( s->emf_iter * s->dt ) ) {
-            TRY( run_shift( s->plan, s->stream, 0 ) );
-            s->emf_mw.advance();
+        unsigned key = 0;
+        bool eager = !s->use_graph || s->profile || !s->jdep_clean || s->species.size() > 30;
+        const unsigned gy = s->nty * s->nxy;
+        for ( size_t k = 0; k < s->species.size() && !eager; k++ ) {
+            HSpecies * h = s->species[k];
+            if ( h->counters_dirty || h->sort_pending ) eager = true;
+            if ( h->mw.needs_move( (float) ( ( h->iter + 1 ) * h->dt ) ) ) {
+                key |= 1u << k;
+                const uint64_t add = h->dens.type == ZPIC_DENSITY_NONE ? 0 : (uint64_t) gy * h->ppc[0] * h->ppc[1];
+                if ( h->np_bound + add > h->max_part ) eager = true;
+            }
         }
-        s->iter++;
+        if ( s->emf_mw.active && s->emf_mw.needs_move( ( s->emf_iter + 1 ) * s->dt ) ) key |= 1u << 31;
+        if ( eager ) { TRY( mw_step( s ) ); continue; }
+        Plan & P = s->plan;
+        const uint64_t l0 = s->launches;
+        auto it = P.mw_graphs.find( key );
+        if ( it == P.mw_graphs.end() ) {
+            cudaGraph_t g;
+            CK( cudaStreamBeginCapture( s->stream, cudaStreamCaptureModeThreadLocal ) );
+            const int rc = mw_step( s );
+            const cudaError_t e = cudaStreamEndCapture( s->stream, &g );
+            if ( rc != ZPIC_OK ) return rc;
+            if ( e != cudaSuccess ) return fail( ZPIC_E_CUDA, std::string( "graph capture: " ) + cudaGetErrorString( e ) );
+            cudaGraphExec_t ge;
+            const int nk = count_graph_kernels( g );
+            const cudaError_t e2 = cudaGraphInstantiate( &ge, g, 0 );
+            cudaGraphDestroy( g );
+            if ( e2 != cudaSuccess ) return fail( ZPIC_E_CUDA, std::string( "graph instantiate: " ) + cudaGetErrorString( e2 ) );
+            it = P.mw_graphs.emplace( key, std::make_pair( ge, nk ) ).first;
+        } else {
+            g_dry = true;
+            const int rc = mw_step( s );
+            g_dry = false;
+            if ( rc != ZPIC_OK ) return rc;
+        }
+        CK( cudaGraphLaunch( it->second.first, s->stream ) );
+        s->launches = l0 + it->second.second;
     }
     return ZPIC_OK;
 }
@@ -1289,6 +1361,16 @@ int zpic_b200_species_nmove( zpic_sim * s, int32_t sp, uint64_t * nmove ) {
     CK( cudaMemcpyAsync( &v, s->species[sp]->d.nmove, sizeof( v ), cudaMemcpyDeviceToHost, s->stream ) );
     CK( cudaStreamSynchronize( s->stream ) );
     *nmove = v;
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_repacks( zpic_sim * s, int32_t sp, uint64_t * repacks ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    if ( !repacks ) return fail( ZPIC_E_INVALID, "null argument" );
+    unsigned long long v = 0;
+    CK( cudaMemcpyAsync( &v, s->species[sp]->d.nmove + 1, sizeof( v ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    *repacks = v;
     return ZPIC_OK;
 }
 

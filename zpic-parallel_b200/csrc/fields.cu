@@ -85,8 +85,33 @@ __device__ __forceinline__ void add_xy( const float * raw, const RunDev & R, int
     }
 }
 
+// The guard-cell copies run one thread per guard cell of every tile of the
+// work list: thread gid handles guard cell gid % per of item gid / per, so
+// the many small, independent copies of all tiles are in flight at once.
+constexpr int GC_THREADS = 256;
+
+// Guard cell g (row-major over the tile's guard region) -> tile cell (i, j):
+// the GL bottom rows, the GU top rows, then the GL left and GU right cells of
+// every interior row.
+__device__ __forceinline__ void guard_cell( int g, const RunDev & R, int & i, int & j ) {
+    const int bottom = GL * R.extx;
+    if ( g < bottom ) { i = g % R.extx; j = g / R.extx; return; }
+    g -= bottom;
+    const int top = GU * R.extx;
+    if ( g < top ) { i = g % R.extx; j = GL + R.nxy + g / R.extx; return; }
+    g -= top;
+    const int c = g % ( GL + GU );
+    j = GL + g / ( GL + GU );
+    i = c < GL ? c : R.nxx + c;
+}
+
+__device__ __forceinline__ int guard_count( const RunDev & R ) { return R.extx * R.exty - R.nxx * R.nxy; }
+
 // Current::advance's add_from_gc + copy_to_gc (current.cpp:227-233) in one
-// pass: Jdep (tile-local deposits) -> J (summed, guard cells refreshed).
+// pass: Jdep (tile-local deposits) -> J (summed, guard cells refreshed).  One
+// CTA per tile: each cell gathers up to nine contributions, and a tile's
+// threads read neighbouring cells together (measured faster than one thread
+// per cell of all tiles for this kernel, unlike the pure copies below).
 __global__ void __launch_bounds__( 128 )
 k_current_gc( const TileItem * __restrict__ items, const RunDev * __restrict__ runs )
 {
@@ -106,47 +131,49 @@ k_current_gc( const TileItem * __restrict__ items, const RunDev * __restrict__ r
 }
 
 // grid::copy_to_gc on E and B in place (axes: 1 x, 2 y, 3 both)
-__global__ void __launch_bounds__( 128 )
-k_emf_gc( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, int axes )
+__global__ void __launch_bounds__( GC_THREADS )
+k_emf_gc( const TileItem * __restrict__ items, int nitems, int per, const RunDev * __restrict__ runs, int axes )
 {
-    const TileItem it = items[ blockIdx.x ];
+    const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x;     // n * per < 2^31 (launcher)
+    const int w = (int) ( gid / (unsigned) per ), g = (int) ( gid % (unsigned) per );
+    if ( w >= nitems ) return;
+    const TileItem it = items[w];
     const RunDev & R = runs[ it.run ];
+    if ( g >= guard_count( R ) ) return;
     const int tx = it.tile % R.ntx, ty = it.tile / R.ntx;
-    const int ncell = R.extx * R.exty;
-    float * E = R.E; float * B = R.B;
-    const size_t base = (size_t) it.tile * R.tile_vol * 3;
-    for ( int c = threadIdx.x; c < ncell; c += blockDim.x ) {
-        const int i = c % R.extx, j = c / R.extx;
-        if ( i >= GL && i < GL + R.nxx && j >= GL && j < GL + R.nxy ) continue;
-        int stx, sty, si, sj;
-        resolve_copy( R, R.emf_perx, R.emf_pery, axes, tx, ty, i, j, stx, sty, si, sj );
-        if ( stx == tx && sty == ty && si == i && sj == j ) continue;
-        const float * e = cellp( E, R, stx, sty, si, sj );
-        const float * b = cellp( B, R, stx, sty, si, sj );
-        E[ base + 3*c ] = e[0]; E[ base + 3*c + 1 ] = e[1]; E[ base + 3*c + 2 ] = e[2];
-        B[ base + 3*c ] = b[0]; B[ base + 3*c + 1 ] = b[1]; B[ base + 3*c + 2 ] = b[2];
-    }
+    int i, j;
+    guard_cell( g, R, i, j );
+    int stx, sty, si, sj;
+    resolve_copy( R, R.emf_perx, R.emf_pery, axes, tx, ty, i, j, stx, sty, si, sj );
+    if ( stx == tx && sty == ty && si == i && sj == j ) return;
+    const size_t dst = ( (size_t) it.tile * R.tile_vol + j * R.extx + i ) * 3;
+    const float * e = cellp( R.E, R, stx, sty, si, sj );
+    const float * b = cellp( R.B, R, stx, sty, si, sj );
+    const float e0 = e[0], e1 = e[1], e2 = e[2], b0 = b[0], b1 = b[1], b2 = b[2];
+    R.E[dst] = e0; R.E[dst + 1] = e1; R.E[dst + 2] = e2;
+    R.B[dst] = b0; R.B[dst + 1] = b1; R.B[dst + 2] = b2;
 }
 
 // J guard-cell refresh only (used after current filters): axes 1 x, 2 y
-__global__ void __launch_bounds__( 128 )
-k_cur_gc( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, int axes )
+__global__ void __launch_bounds__( GC_THREADS )
+k_cur_gc( const TileItem * __restrict__ items, int nitems, int per, const RunDev * __restrict__ runs, int axes )
 {
-    const TileItem it = items[ blockIdx.x ];
+    const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x;     // n * per < 2^31 (launcher)
+    const int w = (int) ( gid / (unsigned) per ), g = (int) ( gid % (unsigned) per );
+    if ( w >= nitems ) return;
+    const TileItem it = items[w];
     const RunDev & R = runs[ it.run ];
+    if ( g >= guard_count( R ) ) return;
     const int tx = it.tile % R.ntx, ty = it.tile / R.ntx;
-    const int ncell = R.extx * R.exty;
-    float * J = R.J;
-    const size_t base = (size_t) it.tile * R.tile_vol * 3;
-    for ( int c = threadIdx.x; c < ncell; c += blockDim.x ) {
-        const int i = c % R.extx, j = c / R.extx;
-        if ( i >= GL && i < GL + R.nxx && j >= GL && j < GL + R.nxy ) continue;
-        int stx, sty, si, sj;
-        resolve_copy( R, R.cur_perx, R.cur_pery, axes, tx, ty, i, j, stx, sty, si, sj );
-        if ( stx == tx && sty == ty && si == i && sj == j ) continue;
-        const float * s = cellp( J, R, stx, sty, si, sj );
-        J[ base + 3*c ] = s[0]; J[ base + 3*c + 1 ] = s[1]; J[ base + 3*c + 2 ] = s[2];
-    }
+    int i, j;
+    guard_cell( g, R, i, j );
+    int stx, sty, si, sj;
+    resolve_copy( R, R.cur_perx, R.cur_pery, axes, tx, ty, i, j, stx, sty, si, sj );
+    if ( stx == tx && sty == ty && si == i && sj == j ) return;
+    const size_t dst = ( (size_t) it.tile * R.tile_vol + j * R.extx + i ) * 3;
+    const float * q = cellp( R.J, R, stx, sty, si, sj );
+    const float q0 = q[0], q1 = q[1], q2 = q[2];
+    R.J[dst] = q0; R.J[dst + 1] = q1; R.J[dst + 2] = q2;
 }
 
 // ---------------------------------------------------------------------------
@@ -536,16 +563,23 @@ namespace zb {
 
 size_t yee_smem_bytes( int tile_vol ) { return (size_t) 9 * tile_vol * sizeof( float ) + 16; }
 
-cudaError_t launch_current_gc( cudaStream_t st, const TileItem * items, int n, const RunDev * runs ) {
+static unsigned gc_blocks( int n, int per ) {
+    return (unsigned) ( ( (long long) n * per + GC_THREADS - 1 ) / GC_THREADS );
+}
+static bool gc_fits( int n, int per ) { return (long long) n * per < ( 1LL << 31 ) - GC_THREADS; }
+// per: guard cells of the largest tile of the list (unused by the current sum)
+cudaError_t launch_current_gc( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int ) {
     if ( n > 0 ) k_current_gc<<< n, 128, 0, st >>>( items, runs );
     return cudaGetLastError();
 }
-cudaError_t launch_emf_gc( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int axes ) {
-    if ( n > 0 ) k_emf_gc<<< n, 128, 0, st >>>( items, runs, axes );
+cudaError_t launch_emf_gc( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int axes, int per ) {
+    if ( !gc_fits( n, per ) ) return cudaErrorInvalidConfiguration;
+    if ( n > 0 ) k_emf_gc<<< gc_blocks( n, per ), GC_THREADS, 0, st >>>( items, n, per, runs, axes );
     return cudaGetLastError();
 }
-cudaError_t launch_cur_gc( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int axes ) {
-    if ( n > 0 ) k_cur_gc<<< n, 128, 0, st >>>( items, runs, axes );
+cudaError_t launch_cur_gc( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int axes, int per ) {
+    if ( !gc_fits( n, per ) ) return cudaErrorInvalidConfiguration;
+    if ( n > 0 ) k_cur_gc<<< gc_blocks( n, per ), GC_THREADS, 0, st >>>( items, n, per, runs, axes );
     return cudaGetLastError();
 }
 cudaError_t launch_yee( cudaStream_t st, const TileItem * items, int n, const RunDev * runs,

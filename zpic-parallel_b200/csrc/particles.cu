@@ -690,7 +690,7 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
     __syncthreads();
     long long pc = block_exscan< PLAN_THREADS >( cap_sum, &s_total );
     for ( int t = t0; t < t1; t++ ) { S.new_off[t] = (int) pc; pc += S.new_cap[t]; }
-    if ( threadIdx.x == 0 ) *S.mode = 1;
+    if ( threadIdx.x == 0 ) { *S.mode = 1; S.nmove[1] += 1; }
 }
 
 __device__ __forceinline__ void copy_particle( const PartArrays & d, size_t di, const PartArrays & s, size_t si ) {
@@ -864,16 +864,25 @@ k_sort_in( const Item * __restrict__ items, int nitems, const SpDev * __restrict
 // The order of the reference's sequential loops (i1, i0, cell) is kept with
 // a block-wide ordered scan.
 // ---------------------------------------------------------------------------
-struct InjRule {
-    int type;                 // 1 uniform, 2 step, 3 slab, 4 sphere
-    int diry;
-    float a, b;               // step pos / slab begin,end (cells)
-    float cx, cy, r2;         // sphere (simulation units)
-    float dxx, dxy;
-    int ppcx, ppcy;
-    int range[4];             // x.lower, x.upper, y.lower, y.upper (global cells)
-    int tx_limit;             // tiles processed along x (reference quirk for dir = y)
-};
+
+// Moving-window injection parameters that depend on the window's position
+// (Injector rule: step position / slab limits / sphere centre relative to the
+// window, density.cpp:418, 677-678, 937-941), computed on the device from a
+// device copy of the window's move count so that a captured step replays
+// with the right values; the count is advanced afterwards.  The arithmetic
+// is the host's: motion = n_move * dx in double, rounded to float.
+__global__ void k_inj_dyn( float * __restrict__ dyn, unsigned * __restrict__ n_move, int type,
+                           float da, float db, float dx0, double mw_dx )
+{
+    const double motion = *n_move * mw_dx;
+    const float refx = (float) motion;
+    float a = 0.f, b = 0.f, cx = 0.f;
+    if ( type == 2 ) a = ( da - refx ) / dx0;
+    else if ( type == 3 ) { a = ( da - refx ) / dx0; b = ( db - refx ) / dx0; }
+    else if ( type == 4 ) cx = da - refx;
+    dyn[0] = a; dyn[1] = b; dyn[2] = cx;
+    *n_move += 1;
+}
 
 __device__ __forceinline__ int inj_test( const InjRule & r, int shiftx, int shifty, int cx, int cy, float posx, float posy ) {
     float t;
@@ -920,6 +929,7 @@ k_inject( int sp, const SpDev * __restrict__ sps, const RunDev * __restrict__ ru
     const int t = blockIdx.x;
     const int tx = t % R.ntx, ty = t / R.ntx;
     const int nxx = R.nxx, nxy = R.nxy;
+    if ( r.dyn ) { r.a = r.dyn[0]; r.b = r.dyn[1]; r.cx = r.dyn[2]; }
     int ri0, ri1, rj0, rj1;
     const bool in_range = ( tx < r.tx_limit ) && inj_tile_range( r, tx, ty, nxx, nxy, ri0, ri1, rj0, rj1 );
     if ( !in_range ) {
@@ -1212,6 +1222,12 @@ cudaError_t launch_sort( cudaStream_t st, const Item * items, int nitems, const 
     const int nb = ( nitems + SORT_WARPS - 1 ) / SORT_WARPS;
     k_sort_out<<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, runs );
     k_sort_in<<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_inj_dyn( cudaStream_t st, float * dyn, unsigned * n_move, int type, float da, float db,
+                            float dx0, double mw_dx ) {
+    k_inj_dyn<<< 1, 1, 0, st >>>( dyn, n_move, type, da, db, dx0, mw_dx );
     return cudaGetLastError();
 }
 

@@ -67,7 +67,7 @@ struct SpDev {
     int * extra;                  // [ntiles] room to reserve for injection (or nullptr)
     int * mode;                   // [1] 0 = in-place sort, 1 = repack
     double * energy;              // [ntiles*nchunk] per work-item kinetic energy sums
-    unsigned long long * nmove;   // pushes counter
+    unsigned long long * nmove;   // [0] pushes counter, [1] repacks of the tile slots
     float alpha;                  // 0.5*dt/m_q (species.cpp:2305)
     float dt_dx, dt_dy;           // dt/dx (species.cpp:2140-2143)
     float q;                      // charge per particle
@@ -171,5 +171,19 @@ struct Item { int sp; int tile; int chunk; int pad; };
 // q1 < 0 for a 1D phase space).  r = lower range bound in deposit units,
 // rdx = bins per unit, norm = weight of one particle.
 struct PhaSpec { int q0, q1, n0, n1; float r0, rdx0, r1, rdx1, norm; int smem; };
+
+// Density injection rule of one species (Injector, density.cpp): which
+// in-cell positions of a global cell range receive a particle.
+struct InjRule {
+    int type;                 // 1 uniform, 2 step, 3 slab, 4 sphere
+    int diry;
+    float a, b;               // step pos / slab begin,end (cells)
+    float cx, cy, r2;         // sphere (simulation units)
+    float dxx, dxy;
+    int ppcx, ppcy;
+    int range[4];             // x.lower, x.upper, y.lower, y.upper (global cells)
+    int tx_limit;             // tiles processed along x (reference quirk for dir = y)
+    const float * dyn;        // if set: a, b, cx computed on the device for the window's position
+};
 
 }  // namespace zb

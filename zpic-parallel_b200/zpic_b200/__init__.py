@@ -40,7 +40,7 @@ EXPORTS = [
     'zpic_b200_sim_phase_times', 'zpic_b200_sim_reset_phase_times', 'zpic_b200_sim_launch_count',
     'zpic_b200_sim_stream',
     'zpic_b200_batch_stream', 'zpic_b200_batch_launch_count',
-    'zpic_b200_sim_autotune', 'zpic_b200_batch_autotune',
+    'zpic_b200_sim_autotune', 'zpic_b200_batch_autotune', 'zpic_b200_species_repacks',
     'zpic_b200_emf_set_bc', 'zpic_b200_emf_advance', 'zpic_b200_emf_energy', 'zpic_b200_laser_add',
     'zpic_b200_current_set_bc', 'zpic_b200_current_set_filter', 'zpic_b200_current_zero',
     'zpic_b200_current_advance',
@@ -119,6 +119,7 @@ def lib():
             'zpic_b200_batch_stream': (I, [P, ctypes.POINTER(P)]),
             'zpic_b200_batch_launch_count': (I, [P, ctypes.POINTER(ctypes.c_uint64)]),
             'zpic_b200_sim_autotune': (I, [P, I, IP]),
+            'zpic_b200_species_repacks': (I, [P, I, U64P]),
             'zpic_b200_batch_autotune': (I, [P, I, IP]),
             'zpic_b200_emf_set_bc': (I, [P, IP]),
             'zpic_b200_emf_advance': (I, [P, I]),
@@ -344,6 +345,12 @@ class Simulation:
     def species_energy(self, sp):
         v = ctypes.c_double()
         _check(lib().zpic_b200_species_energy(self.h, sp, ctypes.byref(v)))
+        return v.value
+
+    def repacks(self, sp):
+        """Times the tile sort rebuilt the slot layout of species sp."""
+        v = ctypes.c_uint64()
+        _check(lib().zpic_b200_species_repacks(self.h, sp, ctypes.byref(v)))
         return v.value
 
     def np_total(self, sp):
