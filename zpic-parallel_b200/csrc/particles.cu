@@ -718,7 +718,7 @@ k_sort_out( const Item * __restrict__ items, int nitems, const SpDev * __restric
     const SpDev & S = sps[ it.sp ];
     const RunDev & R = runs[ S.run ];
     const int mode = *S.mode;
-    if ( mode == 2 ) return;
+    if ( mode != 0 ) return;          // repacks: k_repack_out
     const int t = it.tile;
     const int ntx = R.ntx, nty = R.nty, nxx = R.nxx, nxy = R.nxy;
     const int tx = t % ntx, ty = t / ntx;
@@ -796,37 +796,72 @@ k_sort_out( const Item * __restrict__ items, int nitems, const SpDev * __restric
         }
         __syncwarp();
         if ( lane == 0 ) S.np[t] = n0;
-    } else {
-        // repack: stayers to B at new_off[t] + rank, leavers to B after the
-        // target's stayers.
-        int ns = 0;
-        for ( int i0 = 0; i0 < np; i0 += 32 ) {
-            const int i = i0 + lane;
-            bool stay = false;
-            size_t g = 0;
-            uint32_t c = 0;
-            int xc = 0, yc = 0;
-            if ( i < np ) {
-                g = (size_t) off + i;
-                c = S.A.cell[g];
-                const int ix = cell_x( c ), iy = cell_y( c );
-                xc = ( ix >= nxx ) - ( ix < 0 ); yc = ( iy >= nxy ) - ( iy < 0 );
-                stay = xc == 0 && yc == 0;
-            }
-            const unsigned m = __ballot_sync( 0xffffffffu, stay );
-            if ( stay ) copy_particle( S.B, (size_t) S.new_off[t] + ns + __popc( m & lt ), S.A, g );
-            ns += __popc( m );
-            if ( i < np && !stay ) {
-                const int ttx = wrap_tile( tx + xc, ntx, S.perx ), tty = wrap_tile( ty + yc, nty, S.pery );
-                if ( ttx >= 0 && tty >= 0 ) {
-                    const int tt = tty * ntx + ttx;
-                    const int slot = atomicAdd( S.stage_cnt + tt, 1 );
-                    const size_t d = (size_t) S.new_off[tt] + ( S.np[tt] - S.nidx[tt] ) + slot;
-                    copy_particle( S.B, d, S.A, g );
-                    S.B.cell[d] = pack_cell( cell_x( c ) - xc * nxx, cell_y( c ) - yc * nxy );
+    }
+}
+
+// Repack (sort plan mode 1): every particle of the species goes to buffer B
+// in the new slot layout -- stayers into their own tile's new slot, leavers
+// into their target's -- then B is copied back to A.  These kernels run on a
+// fixed grid of CTAs striding over the whole particle buffer (a tile's
+// particles are spread over all CTAs, however unevenly the tiles are filled)
+// and return at once when no species of the list repacks.  Slots are claimed
+// per destination with one atomic per group of lanes sharing it.
+constexpr int REPACK_THREADS = 256;
+
+__global__ void __launch_bounds__( REPACK_THREADS )
+k_repack_out( const SpDev * __restrict__ sps, const int * __restrict__ species_list, int nspecies,
+              const RunDev * __restrict__ runs )
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = ( 1u << lane ) - 1u;
+    for ( int k = 0; k < nspecies; k++ ) {
+        const SpDev & S = sps[ species_list[k] ];
+        if ( *S.mode != 1 ) continue;
+        const RunDev & R = runs[ S.run ];
+        const int nt = S.ntiles, ntx = R.ntx, nty = R.nty, nxx = R.nxx, nxy = R.nxy;
+        const long long n = S.max_part;
+        for ( long long p0 = (long long) blockIdx.x * blockDim.x; p0 < n; p0 += (long long) gridDim.x * blockDim.x ) {
+            const long long p = p0 + threadIdx.x;
+            int dest = -1, ix = 0, iy = 0, xc = 0, yc = 0;
+            if ( p < n ) {
+                // tile of slot p: the last tile whose slot starts at or before p
+                int lo = 0, hi = nt - 1;
+                while ( lo < hi ) {
+                    const int mid = ( lo + hi + 1 ) >> 1;
+                    if ( S.off[mid] <= p ) lo = mid; else hi = mid - 1;
+                }
+                const int t = lo, i = (int) ( p - S.off[t] );
+                if ( i >= 0 && i < S.np[t] ) {
+                    const uint32_t c = S.A.cell[p];
+                    ix = cell_x( c ); iy = cell_y( c );
+                    xc = ( ix >= nxx ) - ( ix < 0 ); yc = ( iy >= nxy ) - ( iy < 0 );
+                    const int ttx = wrap_tile( t % ntx + xc, ntx, S.perx ), tty = wrap_tile( t / ntx + yc, nty, S.pery );
+                    dest = ( ttx >= 0 && tty >= 0 ) ? tty * ntx + ttx : -1;
                 }
             }
+            const unsigned same = __match_any_sync( 0xffffffffu, dest );
+            const int leader = __ffs( same ) - 1;
+            int base = 0;
+            if ( dest >= 0 && lane == leader ) base = atomicAdd( S.stage_cnt + dest, __popc( same ) );
+            base = __shfl_sync( same, base, leader );
+            if ( dest >= 0 ) {
+                const size_t d = (size_t) S.new_off[dest] + base + __popc( same & lt );
+                copy_particle( S.B, d, S.A, (size_t) p );
+                if ( xc != 0 || yc != 0 ) S.B.cell[d] = pack_cell( ix - xc * nxx, iy - yc * nxy );
+            }
         }
+    }
+}
+
+__global__ void __launch_bounds__( REPACK_THREADS )
+k_repack_in( const SpDev * __restrict__ sps, const int * __restrict__ species_list, int nspecies )
+{
+    for ( int k = 0; k < nspecies; k++ ) {
+        const SpDev & S = sps[ species_list[k] ];
+        if ( *S.mode != 1 ) continue;
+        const long long n = S.max_part;
+        for ( long long p = (long long) blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long) gridDim.x * blockDim.x )
+            copy_particle( S.A, (size_t) p, S.B, (size_t) p );
     }
 }
 
@@ -850,10 +885,8 @@ k_sort_in( const Item * __restrict__ items, int nitems, const SpDev * __restrict
             copy_particle( S.A, (size_t) off + n0 + k, S.S, (size_t) so + k );
         if ( lane == 0 ) S.np[t] = n0 + in;
     } else if ( mode == 1 ) {
-        const int n = S.new_np[t], off = S.new_off[t];
-        for ( int k = lane; k < n; k += 32 )
-            copy_particle( S.A, (size_t) off + k, S.B, (size_t) off + k );
-        if ( lane == 0 ) { S.np[t] = n; S.off[t] = off; S.cap[t] = S.new_cap[t]; }
+        // the particles are in place already (k_repack_out, k_repack_in)
+        if ( lane == 0 ) { S.np[t] = S.new_np[t]; S.off[t] = S.new_off[t]; S.cap[t] = S.new_cap[t]; }
     }
     __syncwarp();
     if ( lane == 0 ) { S.in_cnt[t] = 0; S.nidx[t] = 0; }
@@ -1221,6 +1254,11 @@ cudaError_t launch_sort( cudaStream_t st, const Item * items, int nitems, const 
     k_sort_plan<<< nspecies, PLAN_THREADS, 0, st >>>( sps, species_list, runs, use_extra );
     const int nb = ( nitems + SORT_WARPS - 1 ) / SORT_WARPS;
     k_sort_out<<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, runs );
+    int dev = 0, sms = 148;
+    cudaGetDevice( &dev );
+    cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
+    k_repack_out<<< 4 * sms, REPACK_THREADS, 0, st >>>( sps, species_list, nspecies, runs );
+    k_repack_in<<< 4 * sms, REPACK_THREADS, 0, st >>>( sps, species_list, nspecies );
     k_sort_in<<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps );
     return cudaGetLastError();
 }
