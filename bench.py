@@ -539,6 +539,9 @@ def run_weibel(args, world, rank, local):
     s = zb.Simulation((nt, nt), (32, 32), (nt * 32 * 0.1, nt * 32 * 0.1), 0.07, device=local)
     s.add_species(-1.0, (ppc, ppc), udist=('thermalcorr', (0.1, 0.1, 0.1), (0, 0, 0.6)), name='electrons')
     s.add_species(1.0, (ppc, ppc), udist=('thermalcorr', (0.1, 0.1, 0.1), (0, 0, -0.6)), name='positrons')
+    # the plasma filaments (tiles reach twice the mean occupancy): CTAs in
+    # proportion to each tile's particles
+    s.set_option('chunks', -1)
     npart = s.np_total(0) + s.np_total(1)
     stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -564,7 +567,8 @@ def run_weibel(args, world, rank, local):
             'steps': steps, 'warmup': 0, 'ms_per_step': t / steps * 1e3, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded)',
             'config': {'workload': 'Weibel %dx%d cells, 32x32 tiles, 2 species x 8x8 ppc, %d steps'
-                                   % (nt * 32, nt * 32, steps), 'particles': npart},
+                                   % (nt * 32, nt * 32, steps), 'particles': npart,
+                       'ctas_per_tile': 'in proportion to tile occupancy (chunks -1)'},
             'reference_gpu': ref, 'clocks': clk.summary(),
         }))
     return 0

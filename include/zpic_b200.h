@@ -147,7 +147,9 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
 /*
  * Tuning / instrumentation knobs (no reference counterpart):
  *   "graph"          1/0  capture repeated steps in a CUDA graph (default 1)
- *   "chunks"         n    CTAs per tile in the particle kernel (0 = automatic)
+ *   "chunks"         n    CTAs per tile in the particle kernel: n > 0 for every
+ *                         tile, 0 automatic (default), -1 automatic and in
+ *                         proportion to each tile's particles
  *   "profile"        1/0  record CUDA events around each kernel phase
  *   "jacc"           0/1/2 tile current accumulation in shared memory: 0 FP32
  *                         atomics (the reference's FP32 sums, in another order),
@@ -158,9 +160,10 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  */
 int zpic_b200_sim_set_option( zpic_sim * sim, const char * key, double value );
 /* Autotuner (no reference counterpart): times `steps` steps for each
- * candidate number of CTAs per tile (1, 2, 4, ... 64, at least 256 particles
- * per CTA on average) and keeps the fastest ("chunks" option); *chosen gets
- * it.  The trial steps are real Simulation::advance steps (each candidate
+ * candidate number of CTAs per tile -- the "chunks" values 0 and -1
+ * (automatic; -1 in proportion to each tile's particles) and 1, 2, 4, ... 64
+ * (at least 256 particles per CTA on average) -- and keeps the fastest;
+ * *chosen gets it.  The trial steps are real Simulation::advance steps (each candidate
  * runs 1 + steps of them); the choice changes no result beyond the FP32
  * order in which per-CTA partial currents are added.  Not for moving-window
  * simulations. */

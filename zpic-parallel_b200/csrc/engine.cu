@@ -267,6 +267,25 @@ static int auto_chunks( int ntiles_total, int opt ) {
     return std::min( 64, ( target + ntiles_total - 1 ) / ntiles_total );
 }
 
+// CTAs per tile of the particle kernel ("chunks" option): n > 0 for every
+// tile; 0, the automatic choice, for every tile; -1 balanced: a tile of
+// average occupancy gets the automatic number of CTAs, a fuller tile
+// proportionally more (up to twice as many), a sparser one fewer, so that
+// every CTA moves about the same number of particles however unevenly the
+// plasma fills the tiles (faster once a Weibel plasma has filamented, slower
+// for uniform plasmas and for runs with many empty tiles).
+static void set_chunks( zpic_sim * s ) {
+    int ntot = 0; uint64_t np = 0;
+    for ( auto * h : s->species ) { ntot += h->ntiles; np += h->np_bound; }
+    const int base = auto_chunks( std::max( 1, ntot ), std::max( 0, s->chunks_opt ) );
+    for ( auto * h : s->species ) {
+        if ( s->chunks_opt >= 0 ) { h->d.nchunk = base; h->d.chunk_target = 0; continue; }
+        h->d.nchunk = std::min( 64, 2 * base );
+        const uint64_t per_tile = ( np + ntot - 1 ) / std::max( 1, ntot );
+        h->d.chunk_target = (int) std::max<uint64_t>( 256, ( per_tile + base - 1 ) / base );
+    }
+}
+
 static int upload_run( zpic_sim * s ) {
     RunDev & R = s->run;
     R.emf_perx = s->emf_bc[0] == ZPIC_EMF_BC_PERIODIC; R.emf_pery = s->emf_bc[2] == ZPIC_EMF_BC_PERIODIC;
@@ -317,7 +336,7 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
         for ( size_t k = 0; k < s->species.size(); k++ ) {
             HSpecies * sp = s->species[k];
             SpDev d = sp->d;
-            if ( batch_chunks ) d.nchunk = batch_chunks;
+            if ( batch_chunks ) { d.nchunk = batch_chunks; d.chunk_target = 0; }
             d.run = (int) r;
             const int gi = (int) P.sps_h.size();
             P.sps_h.push_back( d );
@@ -807,8 +826,9 @@ static int species_advance_mw( zpic_sim * s, int sp ) {
 }
 
 // ---- autotuning of CTAs per tile ----
-// Candidates: 1, 2, 4, ... 64 CTAs per tile, keeping at least 256 particles
-// per CTA on average, plus the automatic choice.  Each candidate runs one
+// Candidates: the automatic choices (0 uniform, -1 occupancy-balanced) and
+// 1, 2, 4, ... 64 CTAs per tile, keeping at least 256 particles per CTA on
+// average.  Each candidate runs one
 // untimed step (graph capture) and `steps` timed steps; the trial steps are
 // real steps of the simulation(s).  The physics does not depend on the
 // choice; only the order in which the per-CTA partial currents are added to
@@ -818,7 +838,9 @@ static std::vector<int> chunk_candidates( uint64_t particles, uint64_t tiles, in
     const double per_tile = tiles ? (double) particles / tiles : 0.0;
     for ( int k = 1; k <= 64; k *= 2 )
         if ( k == 1 || per_tile / k >= 256.0 ) c.push_back( k );
-    if ( std::find( c.begin(), c.end(), automatic ) == c.end() ) c.push_back( automatic );
+    (void) automatic;
+    c.insert( c.begin(), -1 );
+    c.insert( c.begin(), 0 );
     return c;
 }
 
@@ -995,9 +1017,8 @@ int zpic_b200_sim_add_species( zpic_sim * s, const zpic_species_desc * desc, int
     s->species.push_back( sp.release() );
     // chunking depends on the total tile count of all species
     int ntot = 0; for ( auto * h : s->species ) ntot += h->ntiles;
-    const int ch = auto_chunks( ntot, s->chunks_opt );
-    for ( auto * h : s->species ) h->d.nchunk = ch;
     TRY( species_upload( s, raw, np, ix.data(), x.data(), u.data() ) );
+    set_chunks( s );
     if ( species_id ) *species_id = (int) s->species.size() - 1;
     return ZPIC_OK;
 }
@@ -1037,10 +1058,8 @@ int zpic_b200_sim_set_option( zpic_sim * s, const char * key, double v ) {
     }
     else if ( k == "chunks" ) {
         // the per-item energy array holds 64 chunks per tile
-        s->chunks_opt = std::min( 64, std::max( 0, (int) v ) );
-        int ntot = 0; for ( auto * h : s->species ) ntot += h->ntiles;
-        const int ch = auto_chunks( std::max( 1, ntot ), s->chunks_opt );
-        for ( auto * h : s->species ) h->d.nchunk = ch;
+        s->chunks_opt = std::min( 64, std::max( -1, (int) v ) );
+        set_chunks( s );
         s->plan.release();
     }
     else return fail( ZPIC_E_INVALID, "unknown option " + k );
@@ -1666,6 +1685,7 @@ int zpic_b200_batch_autotune( zpic_batch * b, int32_t steps, int32_t * chosen ) 
     const int automatic = auto_chunks( (int) std::min<uint64_t>( ntiles, 1u << 30 ), 0 );
     int best = automatic; float best_ms = -1;
     for ( int c : chunk_candidates( np, ntiles, automatic ) ) {
+        if ( c < 0 ) continue;          // a batch chunks all of its runs alike
         b->chunks = c;
         TRY( plan_build( b->plan, b->sims, c ) );
         float ms = 0;

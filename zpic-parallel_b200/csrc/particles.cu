@@ -323,8 +323,10 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
 
     const int np = S.np[ t ];
     const int off = S.off[ t ];
-    const int per = ( ( np + nchunk - 1 ) / nchunk + 3 ) & ~3;
-    const int begin = it.chunk * per;
+    // CTAs in proportion to the tile's particles (balanced chunking)
+    const int nc = S.chunk_target > 0 ? max( 1, min( nchunk, ( np + S.chunk_target - 1 ) / S.chunk_target ) ) : nchunk;
+    const int per = ( ( np + nc - 1 ) / nc + 3 ) & ~3;
+    const int begin = it.chunk < nc ? it.chunk * per : np;
     const int end = min( np, begin + per );
     const int eidx = t * nchunk + it.chunk;
 

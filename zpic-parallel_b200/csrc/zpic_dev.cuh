@@ -52,7 +52,9 @@ struct PartArrays {
 struct SpDev {
     int run;
     int ntiles;
-    int nchunk;                   // CTAs per tile in the particle kernel
+    int nchunk;                   // CTAs per tile in the particle kernel (at most)
+    int chunk_target;             // particles per CTA: a tile uses ceil(np / target) of its
+                                  // nchunk CTAs (0: all of them)
     int max_part;                 // capacity of A and B
     int stage_cap;                // capacity of the staging buffer
     PartArrays A, B, S;
