@@ -29,7 +29,7 @@ size_t yee_smem_bytes( int tile_vol );
 cudaError_t launch_particles( cudaStream_t, int, int, int, const Item *, int, const SpDev *, const RunDev *, const int *,
                               int, int, int );
 cudaError_t launch_sort( cudaStream_t, const Item *, int, const SpDev *, const int *, int, const RunDev *, int );
-cudaError_t launch_inject( cudaStream_t, int, int, const SpDev *, const RunDev *, const InjRule &, int );
+cudaError_t launch_inject( cudaStream_t, int, int, int, int, int, const SpDev *, const RunDev *, const InjRule &, int );
 cudaError_t launch_inj_dyn( cudaStream_t, float *, unsigned *, int, float, float, float, double );
 cudaError_t launch_pack( cudaStream_t, int, int, const SpDev *, const int *, int2 *, float2 *, float * );
 cudaError_t launch_unpack( cudaStream_t, int, int, const SpDev *, const int *, const int2 *, const float2 *, const float * );
@@ -808,12 +808,15 @@ static int species_advance_mw( zpic_sim * s, int sp ) {
             DEV( launch_inj_dyn( s->stream, h->inj_dyn, h->mw_nmove_d, h->dens.type, h->dens.a, h->dens.b,
                                  h->dx[0], h->mw.dx ) );
             r.dyn = h->inj_dyn;
-            DEV( launch_inject( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, r, 1 ) );
+            DEV( cudaMemsetAsync( h->d.extra, 0, h->ntiles * sizeof( int ), s->stream ) );
+            DEV( launch_inject( s->stream, sp, range[0] / s->nxx, range[1] / s->nxx, range[2] / s->nxy, range[3] / s->nxy,
+                                s->plan.sps_d, s->plan.runs_d, r, 1 ) );
             s->launches += 2;
         }
         TRY( species_sort( s, sp, h->dens.type != ZPIC_DENSITY_NONE ) );
         if ( h->dens.type != ZPIC_DENSITY_NONE ) {
-            DEV( launch_inject( s->stream, sp, h->ntiles, s->plan.sps_d, s->plan.runs_d, r, 0 ) );
+            DEV( launch_inject( s->stream, sp, range[0] / s->nxx, range[1] / s->nxx, range[2] / s->nxy, range[3] / s->nxy,
+                                s->plan.sps_d, s->plan.runs_d, r, 0 ) );
             s->launches++;
         }
         h->mw.advance();

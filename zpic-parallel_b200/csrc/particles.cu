@@ -993,11 +993,13 @@ constexpr int INJ_THREADS = 256;
 // count == 1: write the number of particles to inject per tile to S.extra
 // count == 0: inject them after the existing particles of each tile
 __global__ void __launch_bounds__( INJ_THREADS )
-k_inject( int sp, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs, InjRule r, int count )
+k_inject( int sp, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs, InjRule r, int count,
+          int tx0, int ntx_r, int ty0 )
 {
     const SpDev & S = sps[sp];
     const RunDev & R = runs[ S.run ];
-    const int t = blockIdx.x;
+    // CTA b covers tile (tx0 + b % ntx_r, ty0 + b / ntx_r) of the range's tiles
+    const int t = ( ty0 + (int) blockIdx.x / ntx_r ) * R.ntx + tx0 + (int) blockIdx.x % ntx_r;
     const int tx = t % R.ntx, ty = t / R.ntx;
     const int nxx = R.nxx, nxy = R.nxy;
     if ( r.dyn ) { r.a = r.dyn[0]; r.b = r.dyn[1]; r.cx = r.dyn[2]; }
@@ -1315,9 +1317,13 @@ cudaError_t launch_inj_dyn( cudaStream_t st, float * dyn, unsigned * n_move, int
     return cudaGetLastError();
 }
 
-cudaError_t launch_inject( cudaStream_t st, int sp, int ntiles, const SpDev * sps, const RunDev * runs,
-                           const InjRule & r, int count ) {
-    k_inject<<< ntiles, INJ_THREADS, 0, st >>>( sp, sps, runs, r, count );
+// Tiles [tx0, tx1] x [ty0, ty1] hold the injection range; the caller clears
+// the other tiles' counts (count mode).
+cudaError_t launch_inject( cudaStream_t st, int sp, int tx0, int tx1, int ty0, int ty1, const SpDev * sps,
+                           const RunDev * runs, const InjRule & r, int count ) {
+    const int nx = tx1 - tx0 + 1, ny = ty1 - ty0 + 1;
+    if ( nx <= 0 || ny <= 0 ) return cudaSuccess;
+    k_inject<<< nx * ny, INJ_THREADS, 0, st >>>( sp, sps, runs, r, count, tx0, nx, ty0 );
     return cudaGetLastError();
 }
 
