@@ -114,54 +114,74 @@ __device__ __forceinline__ void dudt_boris_euler( float alpha, float ex, float e
 
 // Accumulation of one current contribution into the shared-memory tile
 // current: FP32 or FP64 atomics, or fixed point.  Fixed point: the
-// contribution times js (a power of two that keeps every contribution below
-// 2^31 in magnitude) is rounded to an integer x = hi * 2^16 + lo, and hi
-// (signed) and lo (0..65535) are added to two 32-bit integer accumulators
-// with native shared-memory integer atomics; the lo words sit jlo entries
-// after the hi words.  Integer sums do not depend on the order of the
-// additions; hi and lo sums cannot overflow for up to 2^16 additions per
-// entry, and the kernel flushes the accumulators before that many.
+// contribution arrives already multiplied by js (a power of two that keeps
+// every contribution below 2^31 in magnitude, folded into the charge factors)
+// and is rounded to an integer x; floor(x / 2^16) is added to a hi word and x
+// itself (mod 2^32) to a second word jlo entries later, both with native
+// shared-memory integer atomics.  Integer sums do not depend on the order of
+// the additions; the hi sum cannot overflow and the low parts are recovered
+// exactly for up to 2^16 additions per entry, and the kernel flushes the
+// accumulators before that many.
 struct JAcc { float js; int jlo; };
 __device__ __forceinline__ void jadd( float * p, float v, JAcc ) { atomicAdd( p, v ); }
 __device__ __forceinline__ void jadd( double * p, float v, JAcc ) { atomicAdd( p, (double) v ); }
 __device__ __forceinline__ void jadd( int * p, float v, JAcc a ) {
-    const int x = __float2int_rn( v * a.js );
+    const int x = __float2int_rn( v );
     atomicAdd( p, x >> 16 );
-    atomicAdd( reinterpret_cast<unsigned int *>( p + a.jlo ), (unsigned int) ( x & 0xFFFF ) );
+    atomicAdd( reinterpret_cast<unsigned int *>( p + a.jlo ), (unsigned int) x );
 }
-// value of a fixed-point accumulator pair
-__device__ __forceinline__ double jfix_value( int hi, unsigned int lo, double inv ) {
+// value of a fixed-point accumulator pair: hi = sum of floor(x / 2^16),
+// full = sum of x mod 2^32, so full - hi * 2^16 (mod 2^32) is the sum of the
+// low 16-bit parts, exact below 2^32 (up to 65537 additions).
+__device__ __forceinline__ double jfix_value( int hi, unsigned int full, double inv ) {
+    const unsigned int lo = full - ( (unsigned int) hi << 16 );
     return ( (double) hi * 65536.0 + (double) lo ) * inv;
 }
 
 // Charge-conserving current of one segment inside one cell (species.cpp:267-310),
 // accumulated into the shared-memory tile current with shared atomics.
+// hqx, hqy are half the reference's qnx, qny and qvz its q vz / 2, all times
+// the fixed-point scale for the fixed-point tile current: powers of two, so
+// every in-plane contribution is bit-identical to the reference's.  The
+// out-of-plane weights are regrouped as a (c + d/2) + b (d - c/2) for the
+// fixed-point current (a few roundings apart); FP32 and FP64 tile currents
+// keep the reference's expression.
 template < typename JT >
 __device__ __forceinline__ void dep_current_seg( int ix, int iy, float x0x, float x0y, float x1x, float x1y,
-                                                 float qnxx, float qnxy, float qvz, JT * J, int stride, JAcc ja ) {
+                                                 float hqx, float hqy, float qvz, JT * J, int stride, JAcc ja ) {
     const float S0x0 = 0.5f - x0x, S0x1 = 0.5f + x0x;
     const float S1x0 = 0.5f - x1x, S1x1 = 0.5f + x1x;
     const float S0y0 = 0.5f - x0y, S0y1 = 0.5f + x0y;
     const float S1y0 = 0.5f - x1y, S1y1 = 0.5f + x1y;
-    const float wl1 = qnxx * ( x1x - x0x );
-    const float wl2 = qnxy * ( x1y - x0y );
-    const float wp10 = 0.5f * ( S0y0 + S1y0 ), wp11 = 0.5f * ( S0y1 + S1y1 );
-    const float wp20 = 0.5f * ( S0x0 + S1x0 ), wp21 = 0.5f * ( S0x1 + S1x1 );
+    const float wl1 = hqx * ( x1x - x0x );
+    const float wl2 = hqy * ( x1y - x0y );
     JT * Js = J + 3 * ( ix + stride * iy );
     const int s3 = 3 * stride;
-    jadd( Js + 0,      wl1 * wp10, ja );
-    jadd( Js + 1,      wl2 * wp20, ja );
-    jadd( Js + 2,      qvz * ( S0x0 * S0y0 + S1x0 * S1y0 + ( S0x0 * S1y0 - S1x0 * S0y0 ) / 2.0f ), ja );
-    jadd( Js + 3 + 1,  wl2 * wp21, ja );
-    jadd( Js + 3 + 2,  qvz * ( S0x1 * S0y0 + S1x1 * S1y0 + ( S0x1 * S1y0 - S1x1 * S0y0 ) / 2.0f ), ja );
-    jadd( Js + s3 + 0, wl1 * wp11, ja );
-    jadd( Js + s3 + 2, qvz * ( S0x0 * S0y1 + S1x0 * S1y1 + ( S0x0 * S1y1 - S1x0 * S0y1 ) / 2.0f ), ja );
-    jadd( Js + s3 + 5, qvz * ( S0x1 * S0y1 + S1x1 * S1y1 + ( S0x1 * S1y1 - S1x1 * S0y1 ) / 2.0f ), ja );
+    jadd( Js + 0,      wl1 * ( S0y0 + S1y0 ), ja );
+    jadd( Js + 1,      wl2 * ( S0x0 + S1x0 ), ja );
+    jadd( Js + 3 + 1,  wl2 * ( S0x1 + S1x1 ), ja );
+    jadd( Js + s3 + 0, wl1 * ( S0y1 + S1y1 ), ja );
+    if constexpr ( std::is_same<JT, int>::value ) {
+        const float qp0 = qvz * __fmaf_rn( S1y0, 0.5f, S0y0 ), qq0 = qvz * __fmaf_rn( S0y0, -0.5f, S1y0 );
+        const float qp1 = qvz * __fmaf_rn( S1y1, 0.5f, S0y1 ), qq1 = qvz * __fmaf_rn( S0y1, -0.5f, S1y1 );
+        jadd( Js + 2,      __fmaf_rn( S0x0, qp0, S1x0 * qq0 ), ja );
+        jadd( Js + 3 + 2,  __fmaf_rn( S0x1, qp0, S1x1 * qq0 ), ja );
+        jadd( Js + s3 + 2, __fmaf_rn( S0x0, qp1, S1x0 * qq1 ), ja );
+        jadd( Js + s3 + 5, __fmaf_rn( S0x1, qp1, S1x1 * qq1 ), ja );
+    } else {
+        jadd( Js + 2,      qvz * ( S0x0 * S0y0 + S1x0 * S1y0 + ( S0x0 * S1y0 - S1x0 * S0y0 ) / 2.0f ), ja );
+        jadd( Js + 3 + 2,  qvz * ( S0x1 * S0y0 + S1x1 * S1y0 + ( S0x1 * S1y0 - S1x1 * S0y0 ) / 2.0f ), ja );
+        jadd( Js + s3 + 2, qvz * ( S0x0 * S0y1 + S1x0 * S1y1 + ( S0x0 * S1y1 - S1x0 * S0y1 ) / 2.0f ), ja );
+        jadd( Js + s3 + 5, qvz * ( S0x1 * S0y1 + S1x1 * S1y1 + ( S0x1 * S1y1 - S1x1 * S0y1 ) / 2.0f ), ja );
+    }
 }
 
 // Split the trajectory of a particle that crosses at least one cell edge into
 // two or three single-cell segments and deposit them (species.cpp:336-430
 // split2d, crossing cases).  x1 = x0 + (dx, dy) before the cell correction.
+// The split fractions use the approximate division __fdividef (2 ulp): they
+// only place the split point on the cell edge, and the particle's own move
+// stays exact.
 template < typename JT >
 __device__ __forceinline__ void deposit_crossing( int ix, int iy, float x0x, float x0y, float x1x, float x1y,
                                                   float dx, float dy, float qvz, float qnxx, float qnxy,
@@ -169,52 +189,42 @@ __device__ __forceinline__ void deposit_crossing( int ix, int iy, float x0x, flo
     const int dix = ( ( x1x >= 0.5f ) - ( x1x < -0.5f ) );
     const int diy = ( ( x1y >= 0.5f ) - ( x1y < -0.5f ) );
     const int crossx = dix != 0, crossy = diy != 0;
-    int v0x = ix, v0y = iy;  float v0x0 = x0x, v0y0 = x0y, v0x1 = x1x, v0y1 = x1y, v0q = qvz;
-    int v1x = 0, v1y = 0;    float v1x0 = 0, v1y0 = 0, v1x1 = 0, v1y1 = 0, v1q = 0;
+    // first split: on x when x is crossed, else on y (selects, no branch)
+    const float a0 = crossx ? x0x : x0y, b0 = crossx ? x0y : x0x;
+    const float da = crossx ? dx : dy, db = crossx ? dy : dx;
+    const float aint = crossx ? 0.5f * dix : 0.5f * diy;
+    float eps = __fdividef( aint - a0, da );
+    const float bint = b0 + db * eps;
+    const float xint = crossx ? aint : bint, yint = crossx ? bint : aint;
+    int v0x = ix, v0y = iy;  float v0x0 = x0x, v0y0 = x0y, v0x1 = xint, v0y1 = yint, v0q = qvz * eps;
+    int v1x = ix + ( crossx ? dix : 0 ), v1y = iy + ( crossx ? 0 : diy );
+    float v1x0 = crossx ? -xint : xint, v1y0 = crossx ? yint : -yint;
+    float v1x1 = crossx ? x1x - dix : x1x, v1y1 = crossx ? x1y : x1y - diy;
+    float v1q = qvz * ( 1 - eps );
     int v2x = 0, v2y = 0;    float v2x0 = 0, v2y0 = 0, v2x1 = 0, v2y1 = 0, v2q = 0;
-    if ( crossy && !crossx ) {
-        const float yint = 0.5f * diy;
-        const float eps = ( yint - x0y ) / dy;
-        const float xint = x0x + dx * eps;
-        v0x1 = xint; v0y1 = yint; v0q = qvz * eps;
-        v1x = ix; v1y = iy + diy;
-        v1x0 = xint; v1y0 = -yint;
-        v1x1 = x1x; v1y1 = x1y - diy;
-        v1q = qvz * ( 1 - eps );
-    }
-    if ( crossx ) {
-        const float xint = 0.5f * dix;
-        float eps = ( xint - x0x ) / dx;
-        const float yint = x0y + dy * eps;
-        v0x1 = xint; v0y1 = yint; v0q = qvz * eps;
-        v1x = ix + dix; v1y = iy;
-        v1x0 = -xint; v1y0 = yint;
-        v1x1 = x1x - dix; v1y1 = x1y;
-        v1q = qvz * ( 1 - eps );
-        if ( crossy ) {
-            const float yint2 = 0.5f * diy;
-            if ( yint >= -0.5f && yint < 0.5f ) {
-                eps = ( yint2 - yint ) / ( x1y - yint );
-                const float xint2 = -xint + ( x1x - xint ) * eps;
-                v2x = v1x; v2y = v1y + diy;
-                v2x0 = xint2; v2y0 = -yint2;
-                v2x1 = v1x1; v2y1 = v1y1 - diy;
-                v2q = v1q * ( 1 - eps );
-                v1x1 = xint2; v1y1 = yint2;
-                v1q *= eps;
-            } else {
-                eps = ( yint2 - x0y ) / ( yint - x0y );
-                const float xint2 = x0x + ( xint - x0x ) * eps;
-                v2x = v0x; v2y = v0y + diy;
-                v2x0 = xint2; v2y0 = -yint2;
-                v2x1 = v0x1; v2y1 = v0y1 - diy;
-                v2q = v0q * ( 1 - eps );
-                v0x1 = xint2; v0y1 = yint2;
-                v0q *= eps;
-                v1y += diy;
-                v1y0 -= diy;
-                v1y1 -= diy;
-            }
+    if ( crossx && crossy ) {
+        const float yint2 = 0.5f * diy;
+        if ( yint >= -0.5f && yint < 0.5f ) {
+            eps = __fdividef( yint2 - yint, x1y - yint );
+            const float xint2 = -xint + ( x1x - xint ) * eps;
+            v2x = v1x; v2y = v1y + diy;
+            v2x0 = xint2; v2y0 = -yint2;
+            v2x1 = v1x1; v2y1 = v1y1 - diy;
+            v2q = v1q * ( 1 - eps );
+            v1x1 = xint2; v1y1 = yint2;
+            v1q *= eps;
+        } else {
+            eps = __fdividef( yint2 - x0y, yint - x0y );
+            const float xint2 = x0x + ( xint - x0x ) * eps;
+            v2x = v0x; v2y = v0y + diy;
+            v2x0 = xint2; v2y0 = -yint2;
+            v2x1 = v0x1; v2y1 = v0y1 - diy;
+            v2q = v0q * ( 1 - eps );
+            v0x1 = xint2; v0y1 = yint2;
+            v0q *= eps;
+            v1y += diy;
+            v1y0 -= diy;
+            v1y1 -= diy;
         }
     }
     dep_current_seg( v0x, v0y, v0x0, v0y0, v0x1, v0y1, qnxx, qnxy, v0q, J, stride, ja );
@@ -273,18 +283,18 @@ constexpr int FLUSH_PARTICLES = 16384;      // particles between fixed-point flu
 static_assert( FLUSH_PARTICLES % ( PK_PPT * PK_THREADS ) == 0, "flush groups hold whole blocks" );
 
 // Adds the fixed-point tile current accumulated so far (hi words at acc[0, n),
-// lo words at acc[n, 2n)) to the raw current of the tile and clears it.  Out
+// full words at acc[n, 2n)) to the raw current of the tile and clears it.  Out
 // of line: it runs once per FLUSH_PARTICLES particles of a CTA, at most.
 __device__ __noinline__ void jfix_flush( int * acc, int n, float * __restrict__ dst, double inv ) {
     __syncthreads();
-    unsigned int * lo = reinterpret_cast<unsigned int *>( acc ) + n;
+    unsigned int * full = reinterpret_cast<unsigned int *>( acc ) + n;
     for ( int i = threadIdx.x; i < n; i += blockDim.x ) {
         const int h = acc[i];
-        const unsigned int l = lo[i];
+        const unsigned int l = full[i];
         if ( h != 0 || l != 0 ) {
             atomicAdd( dst + i, (float) jfix_value( h, l, inv ) );
             acc[i] = 0;
-            lo[i] = 0;
+            full[i] = 0;
         }
     }
     __syncthreads();
@@ -370,9 +380,14 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     const int rxu = ( MOVE && tx != 0 && tx == R.ntx - 1 && ( S.bc[0] > 1 || S.bc[1] > 1 ) && S.bc[1] == 2 );
     const int ryl = ( MOVE && ty == 0 && ( S.bc[2] > 1 || S.bc[3] > 1 ) && S.bc[2] == 2 );
     const int ryu = ( MOVE && ty != 0 && ty == R.nty - 1 && ( S.bc[2] > 1 || S.bc[3] > 1 ) && S.bc[3] == 2 );
+    const bool walls = ( rxl | rxu | ryl | ryu ) != 0;
 
     const float alpha = S.alpha;
-    const float dt_dx = S.dt_dx, dt_dy = S.dt_dy, q = S.q, qnxx = S.qnx, qnxy = S.qny;
+    // current factors: half of q dx / dt, and q / 2 (for q vz / 2), times the
+    // fixed-point scale (exact power-of-two products)
+    const float jsf = FIX ? S.jscale : 1.0f;
+    const float dt_dx = S.dt_dx, dt_dy = S.dt_dy, qhalf = 0.5f * S.q * jsf;
+    const float qnxx = 0.5f * S.qnx * jsf, qnxy = 0.5f * S.qny * jsf;
     const JAcc ja = { S.jscale, 3 * tv };
 
     uint32_t * __restrict__ pc = S.A.cell + off;
@@ -420,7 +435,12 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                     // Sorted particles sit inside their tile; anything else (only
                     // reachable by moving twice without a sort) is flagged and left
                     // untouched so no field or current access leaves the tile block.
-                    if ( ( PUSH || MOVE ) && ( ix < 0 || ix >= nxx || iy < 0 || iy >= nxy ) ) {
+                    // TN x TN tiles (TN a power of two): both 16-bit cell
+                    // coordinates inside [0, TN) exactly when no bit above TN - 1 is set
+                    const bool bad = ( TN > 0 && ( TN & ( TN - 1 ) ) == 0 )
+                                   ? ( c[k] & ~( (uint32_t) ( TN - 1 ) * 0x10001u ) ) != 0
+                                   : ( ix < 0 || ix >= nxx || iy < 0 || iy >= nxy );
+                    if ( ( PUSH || MOVE ) && bad ) {
                         atomicOr( R.status, ST_BAD_CELL );
                         valid = false;
                     }
@@ -441,7 +461,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                         const int dix = ( ( x1x >= 0.5f ) - ( x1x < -0.5f ) );
                         const int diy = ( ( x1y >= 0.5f ) - ( x1y < -0.5f ) );
                         if ( MOVE == 2 ) {
-                            qz = q * u2[k] * rg * 0.5f;
+                            qz = qhalf * u2[k] * rg;
                             cross = ( dix | diy ) != 0;
                             if ( !cross )
                                 dep_current_seg( ix, iy, x0[k], x1[k], x1x, x1y, qnxx, qnxy, qz, Jc, ys, ja );
@@ -449,10 +469,12 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                         ox = x0[k]; oy = x1[k]; oix = ix; oiy = iy;
                         x0[k] = x1x - dix; x1[k] = x1y - diy;
                         ix += dix + shift; iy += diy;
-                        if ( rxl && ix < 0 )    { ix += 1; x0[k] = -x0[k]; u0[k] = -u0[k]; }
-                        if ( rxu && ix >= nxx ) { ix -= 1; x0[k] = -x0[k]; u0[k] = -u0[k]; }
-                        if ( ryl && iy < 0 )    { iy += 1; x1[k] = -x1[k]; u1[k] = -u1[k]; }
-                        if ( ryu && iy >= nxy ) { iy -= 1; x1[k] = -x1[k]; u1[k] = -u1[k]; }
+                        if ( walls ) {
+                            if ( rxl && ix < 0 )    { ix += 1; x0[k] = -x0[k]; u0[k] = -u0[k]; }
+                            if ( rxu && ix >= nxx ) { ix -= 1; x0[k] = -x0[k]; u0[k] = -u0[k]; }
+                            if ( ryl && iy < 0 )    { iy += 1; x1[k] = -x1[k]; u1[k] = -u1[k]; }
+                            if ( ryu && iy >= nxy ) { iy -= 1; x1[k] = -x1[k]; u1[k] = -u1[k]; }
+                        }
                         c[k] = pack_cell( ix, iy );
                     }
                     if ( DETECT ) {
