@@ -212,11 +212,18 @@ def run_reference(args, world, rank):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def make_sim(zb, ncell, device):
+def apply_options(s, args):
+    """Library options given on the command line (default: the library's)."""
+    if getattr(args, 'reorder', None) is not None:
+        s.set_option('reorder', args.reorder)
+    return s
+
+
+def make_sim(zb, ncell, device, args=None):
     nt = ncell // TILE
     s = zb.Simulation((nt, nt), (TILE, TILE), (ncell * DX, ncell * DX), DT, device=device)
     s.add_species(-1.0, (PPC, PPC), udist=('thermal', (UTH, UTH, UTH), (0, 0, 0)))
-    return s
+    return apply_options(s, args)
 
 
 def run_gpu(args, world, rank, local):
@@ -226,7 +233,7 @@ def run_gpu(args, world, rank, local):
 
     torch.cuda.set_device(local)
     ncell = args.cells
-    sim = make_sim(zb, ncell, local)
+    sim = make_sim(zb, ncell, local, args)
     np_total = sim.np_total(0)
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=local)
 
@@ -370,7 +377,7 @@ def run_ensemble(args, world, rank, local):
         s = zb.Simulation((n // TILE, n // TILE), (TILE, TILE), (n * DX, n * DX), DT, device=local)
         s.add_species(-1.0, (p, p), udist=('thermalcorr', (uth, uth, uth), (0, 0, uz)))
         s.add_species(1.0, (p, p), udist=('thermalcorr', (uth, uth, uth), (0, 0, -uz)))
-        sims.append(s)
+        sims.append(apply_options(s, args))
     nparticles = sum(s.np_total(0) + s.np_total(1) for s in sims)
     batch = zb.Batch(sims)
     # device timing: events on one stream that every participating stream
@@ -467,6 +474,7 @@ def run_lwfa(args, world, rank, local):
     s.add_species(-1.0, (4, 2), density=('step', 1.0, 20.0, 0))
     s.add_laser('gaussian', start=17.0, fwhm=2.0, a0=2.0, omega0=10.0, W0=4.0, focus=20.0, axis=25.6, sin_pol=1)
     s.set_moving_window()
+    apply_options(s, args)
     np0 = s.np_total(0)
     stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
     steps = args.steps if args.steps_given else 2000
@@ -542,6 +550,7 @@ def run_weibel(args, world, rank, local):
     # the plasma filaments (tiles reach twice the mean occupancy): CTAs in
     # proportion to each tile's particles
     s.set_option('chunks', -1)
+    apply_options(s, args)
     npart = s.np_total(0) + s.np_total(1)
     stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -589,6 +598,8 @@ def main():
     ap.add_argument('--ref-steps', type=int, default=10)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--autotune', type=int, default=1, help='ensemble: autotune CTAs per tile first (1/0)')
+    ap.add_argument('--reorder', type=int, default=None,
+                    help='steps between in-tile particle reorders (library option "reorder"; default: the library default)')
     args = ap.parse_args()
     args.steps_given = any(a.startswith('--steps') for a in sys.argv[1:])
     args.warmup = max(3, args.warmup)

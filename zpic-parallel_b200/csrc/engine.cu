@@ -38,6 +38,7 @@ cudaError_t launch_dep_charge( cudaStream_t, int, int, const SpDev *, const RunD
 cudaError_t launch_phasespace( cudaStream_t, int, int, const SpDev *, const RunDev *, PhaSpec, float * );
 cudaError_t launch_energy_sum( cudaStream_t, const SpDev *, int, int, double * );
 cudaError_t launch_np_stats( cudaStream_t, const SpDev *, int, unsigned long long * );
+cudaError_t launch_reorder( cudaStream_t, const Item *, int, const SpDev *, const RunDev *, int );
 cudaError_t launch_current_gc( cudaStream_t, const TileItem *, int, const RunDev *, int );
 cudaError_t launch_emf_gc( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
 cudaError_t launch_cur_gc( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
@@ -107,6 +108,9 @@ constexpr int MAX_SPECIES = 64;     // species per simulation
 
 enum Phase { PH_PARTICLES = 0, PH_SORT, PH_CURRENT, PH_FIELDS, PH_OTHER, PH_N };
 
+// Steps between in-tile reorders of the particles (option "reorder").
+constexpr int REORDER_DEFAULT = 0;
+
 // ---------------------------------------------------------------------------
 // species
 // ---------------------------------------------------------------------------
@@ -168,6 +172,9 @@ struct Plan {
     int max_cells = 0, max_guard = 0;   // cells and guard cells of the largest tile
     int jacc = 0;                   // tile current accumulation (option "jacc")
     int tile_n = 0;                 // n when every run has n x n tiles with a specialised kernel
+    int max_tile_cells = 0;         // cells of the largest tile (without guard cells)
+    int reorder_every = 0;          // steps between in-tile reorders (option "reorder"; 0: never)
+    int reorder_count = 0;          // steps since the last reorder
     bool needs_bc_or_filter = false;
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
@@ -214,6 +221,7 @@ struct zpic_sim {
     Plan plan;
     // options
     bool use_graph = true;
+    int reorder_every = REORDER_DEFAULT;
     int chunks_opt = 0;
     int jacc = 2;                   // fixed-point tile current (option "jacc")
     bool profile = false;
@@ -306,7 +314,8 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
     P.sps_h.clear(); P.sp_sim.clear(); P.sp_local.clear();
     P.sp_k1_off.clear(); P.sp_k1_n.clear(); P.sp_sort_off.clear(); P.sp_sort_n.clear();
     P.max_tile_vol = 0;
-    P.max_cells = 0; P.max_guard = 0;
+    P.max_cells = 0; P.max_guard = 0; P.max_tile_cells = 0;
+    P.reorder_every = 0; P.reorder_count = 0;
     P.jacc = -1;
     P.tile_n = -1;
     P.needs_bc_or_filter = false;
@@ -322,6 +331,10 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
         P.max_tile_vol = std::max( P.max_tile_vol, s->run.tile_vol );
         P.max_cells = std::max( P.max_cells, s->run.extx * s->run.exty );
         P.max_guard = std::max( P.max_guard, s->run.extx * s->run.exty - s->run.nxx * s->run.nxy );
+        P.max_tile_cells = std::max( P.max_tile_cells, s->run.nxx * s->run.nxy );
+        // a batch reorders as often as its most frequent run asks
+        if ( s->reorder_every > 0 )
+            P.reorder_every = P.reorder_every > 0 ? std::min( P.reorder_every, s->reorder_every ) : s->reorder_every;
         // one accumulation mode per plan: the runs' own when they agree
         P.jacc = ( P.jacc < 0 || P.jacc == s->jacc ) ? s->jacc : 2;
         const int tn = ( s->nxx == 16 && s->nxy == 16 ) ? 16 : 0;
@@ -559,6 +572,17 @@ static int count_graph_kernels( cudaGraph_t g ) {
     return k;
 }
 
+// In-tile reorder of every species after a complete step, every
+// reorder_every steps (the particles' order only; no physics changes).
+static int maybe_reorder( Plan & P, cudaStream_t st, uint64_t * launches ) {
+    if ( P.reorder_every <= 0 || ++P.reorder_count < P.reorder_every ) return ZPIC_OK;
+    P.reorder_count = 0;
+    PhaseScope ps( prof_sim( P ), st, PH_OTHER, 0 );
+    CK( launch_reorder( st, P.sort_items_d, P.n_sort, P.sps_d, P.runs_d, P.max_tile_cells ) );
+    if ( launches ) *launches += 1;
+    return ZPIC_OK;
+}
+
 static int plan_advance( Plan & P, cudaStream_t st, int nsteps, bool use_graph, uint64_t * launches ) {
     for ( auto * s : P.sims ) TRY( ensure_jdep_clean( s, st ) );
     const bool can_graph = use_graph && nsteps > 1;
@@ -588,6 +612,7 @@ static int plan_advance( Plan & P, cudaStream_t st, int nsteps, bool use_graph, 
             TRY( plan_step_device( P, st ) );
         }
         plan_step_host( P );
+        TRY( maybe_reorder( P, st, launches ) );
     }
     return ZPIC_OK;
 }
@@ -1059,6 +1084,12 @@ int zpic_b200_sim_set_option( zpic_sim * s, const char * key, double v ) {
         if ( j < 0 || j > 2 || j != v ) return fail( ZPIC_E_INVALID, "jacc must be 0, 1 or 2" );
         if ( j != s->jacc ) { s->jacc = j; s->plan.release(); }
     }
+    else if ( k == "reorder" ) {
+        const int r = (int) v;
+        if ( r < 0 || r != v ) return fail( ZPIC_E_INVALID, "reorder must be a step count >= 0" );
+        s->reorder_every = r;
+        s->plan.release();
+    }
     else if ( k == "chunks" ) {
         // the per-item energy array holds 64 chunks per tile
         s->chunks_opt = std::min( 64, std::max( -1, (int) v ) );
@@ -1132,7 +1163,13 @@ int zpic_b200_sim_advance_mov_window( zpic_sim * s, int32_t nsteps ) {
             }
         }
         if ( s->emf_mw.active && s->emf_mw.needs_move( ( s->emf_iter + 1 ) * s->dt ) ) key |= 1u << 31;
-        if ( eager ) { TRY( mw_step( s ) ); continue; }
+        if ( eager ) {
+            TRY( mw_step( s ) );
+            uint64_t l = 0;
+            TRY( maybe_reorder( s->plan, s->stream, &l ) );
+            s->launches += l;
+            continue;
+        }
         Plan & P = s->plan;
         const uint64_t l0 = s->launches;
         auto it = P.mw_graphs.find( key );
@@ -1157,6 +1194,9 @@ int zpic_b200_sim_advance_mov_window( zpic_sim * s, int32_t nsteps ) {
         }
         CK( cudaGraphLaunch( it->second.first, s->stream ) );
         s->launches = l0 + it->second.second;
+        uint64_t l = 0;
+        TRY( maybe_reorder( P, s->stream, &l ) );
+        s->launches += l;
     }
     return ZPIC_OK;
 }

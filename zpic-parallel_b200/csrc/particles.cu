@@ -412,7 +412,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
         }
         const int gend = min( end, g0 + FLUSH_PARTICLES );
         for ( int b0 = g0; b0 < gend; b0 += PK_PPT * PK_THREADS ) {
-            uint32_t c[PK_PPT]; float x0[PK_PPT], x1[PK_PPT], u0[PK_PPT], u1[PK_PPT], u2[PK_PPT];
+            uint32_t c[PK_PPT] = {}; float x0[PK_PPT], x1[PK_PPT], u0[PK_PPT], u1[PK_PPT], u2[PK_PPT];
             int leave_dir[PK_PPT];
 #pragma unroll
             for ( int k = 0; k < PK_PPT; k++ ) {
@@ -430,20 +430,23 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                 leave_dir[k] = 4;
                 int ix = 0, iy = 0, oix = 0, oiy = 0;
                 float d0 = 0.f, d1 = 0.f, qz = 0.f, ox = 0.f, oy = 0.f;
-                if ( valid ) {
+                if ( PUSH || MOVE ) {
                     ix = cell_x( c[k] ); iy = cell_y( c[k] );
                     // Sorted particles sit inside their tile; anything else (only
                     // reachable by moving twice without a sort) is flagged and left
                     // untouched so no field or current access leaves the tile block.
                     // TN x TN tiles (TN a power of two): both 16-bit cell
                     // coordinates inside [0, TN) exactly when no bit above TN - 1 is set
-                    const bool bad = ( TN > 0 && ( TN & ( TN - 1 ) ) == 0 )
+                    const bool bad = valid && ( ( TN > 0 && ( TN & ( TN - 1 ) ) == 0 )
                                    ? ( c[k] & ~( (uint32_t) ( TN - 1 ) * 0x10001u ) ) != 0
-                                   : ( ix < 0 || ix >= nxx || iy < 0 || iy >= nxy );
-                    if ( ( PUSH || MOVE ) && bad ) {
-                        atomicOr( R.status, ST_BAD_CELL );
-                        valid = false;
+                                   : ( ix < 0 || ix >= nxx || iy < 0 || iy >= nxy ) );
+                    const unsigned mbad = __ballot_sync( 0xffffffffu, bad );
+                    if ( mbad ) {
+                        if ( lane == __ffs( mbad ) - 1 ) atomicOr( R.status, ST_BAD_CELL );
+                        valid = valid && !bad;
                     }
+                } else if ( valid ) {
+                    ix = cell_x( c[k] ); iy = cell_y( c[k] );
                 }
                 if ( valid ) {
                     if ( PUSH ) {
@@ -1254,6 +1257,131 @@ __global__ void k_np_stats( const SpDev * __restrict__ sps, int sp, unsigned lon
     }
 }
 
+// ---------------------------------------------------------------------------
+// In-tile reorder (option "reorder": every n steps)
+// ---------------------------------------------------------------------------
+// Particles keep their slot while they move between the cells of their tile,
+// so after some tens of steps the 32 lanes of a warp of the particle kernel
+// hold particles in random cells of the tile, and its shared-memory field
+// gathers and tile-current atomics meet about 3.5-way bank conflicts instead of
+// the 2-way of the injection order.  This kernel puts each tile back into
+// cell round-robin order: particles sorted by (rank within their cell, cell),
+// so round r lists one particle of every cell that holds more than r, in
+// ascending cell order, and consecutive lanes again see consecutive cells.
+// The rank comes from a shared-memory counter per cell (its order between
+// particles of one cell is arbitrary; the ranks are kept in the leaver index
+// list, free between steps); the position of (r, c) is the number of
+// particles in the rounds before r plus the cells before c in round r,
+// counted with a bit mask of the cells present in each round.  The tile is
+// then permuted in place one particle array at a time through shared memory
+// (coalesced loads and stores, 8 bytes of traffic per particle and array).
+// One CTA per tile; tiles with more particles than fit in shared memory, with
+// more particles in one cell than there are rounds, or with a particle outside
+// the tile are left as they are.
+constexpr int RO_THREADS = 1024;
+
+__global__ void __launch_bounds__( RO_THREADS, 1 )
+k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs,
+           int max_rounds, int np_max )
+{
+    extern __shared__ __align__( 16 ) unsigned char smem_raw[];
+    const Item it = items[ blockIdx.x ];
+    const SpDev & S = sps[ it.sp ];
+    const RunDev & R = runs[ S.run ];
+    const int t = it.tile;
+    const int np = S.np[t];
+    if ( np < 64 || np > np_max ) return;
+    const size_t off = S.off[t];
+    const int nxx = R.nxx, nxy = R.nxy, ncell = nxx * nxy;
+    const int ncw = ( ncell + 31 ) >> 5;
+    // shared memory: [buf: np_max words][inv: np_max 16-bit][cnt: ncw*32][base: max_rounds+1]
+    //                [flags: 4][masks: max_rounds*ncw words][word prefix: max_rounds*ncw 16-bit]
+    uint32_t * buf = reinterpret_cast<uint32_t *>( smem_raw );
+    uint16_t * inv = reinterpret_cast<uint16_t *>( buf + np_max );
+    int * cnt = reinterpret_cast<int *>( inv + np_max );
+    int * base = cnt + ncw * 32;
+    int * flags = base + max_rounds + 1;
+    uint32_t * masks = reinterpret_cast<uint32_t *>( flags + 4 );
+    uint16_t * wpre = reinterpret_cast<uint16_t *>( masks + max_rounds * ncw );
+    int * rank = S.idx + off;
+
+    for ( int c = threadIdx.x; c < ncw * 32; c += blockDim.x ) cnt[c] = 0;
+    if ( threadIdx.x == 0 ) { flags[0] = 0; flags[1] = 0; }
+    __syncthreads();
+    for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
+        const uint32_t cl = S.A.cell[ off + i ];
+        const int ix = cell_x( cl ), iy = cell_y( cl );
+        if ( ix < 0 || ix >= nxx || iy < 0 || iy >= nxy ) { flags[0] = 1; continue; }
+        const int r = atomicAdd( cnt + ix + nxx * iy, 1 );
+        rank[i] = r;
+        if ( r >= max_rounds ) flags[0] = 1;
+        else atomicMax( flags + 1, r + 1 );
+    }
+    __syncthreads();
+    if ( flags[0] ) return;
+    const int nround = flags[1];
+    // cells present in each round, one 32-cell word per warp pass
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for ( int w = warp; w < ncw; w += nwarp ) {
+        const int n = cnt[ w * 32 + lane ];
+        for ( int r = 0; r < nround; r++ ) {
+            const uint32_t m = __ballot_sync( 0xffffffffu, n > r );
+            if ( lane == 0 ) masks[ r * ncw + w ] = m;
+        }
+    }
+    __syncthreads();
+    // per round: prefix of the word populations, and the round's size
+    for ( int r = threadIdx.x; r < nround; r += blockDim.x ) {
+        int a = 0;
+        for ( int w = 0; w < ncw; w++ ) { wpre[ r * ncw + w ] = (uint16_t) a; a += __popc( masks[ r * ncw + w ] ); }
+        base[r] = a;
+    }
+    __syncthreads();
+    if ( warp == 0 ) {
+        // exclusive scan of the round sizes, 32 rounds per pass
+        int carry = 0;
+        for ( int r0 = 0; r0 < nround; r0 += 32 ) {
+            const int r = r0 + lane;
+            const int v = r < nround ? base[r] : 0;
+            int incl = v;
+#pragma unroll
+            for ( int o = 1; o < 32; o <<= 1 ) {
+                const int y = __shfl_up_sync( 0xffffffffu, incl, o );
+                if ( lane >= o ) incl += y;
+            }
+            if ( r < nround ) base[r] = carry + incl - v;
+            carry += __shfl_sync( 0xffffffffu, incl, 31 );
+        }
+    }
+    __syncthreads();
+    for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
+        const uint32_t cl = S.A.cell[ off + i ];
+        const int c = cell_x( cl ) + nxx * cell_y( cl );
+        const int r = rank[i];
+        const int w = c >> 5;
+        const int pos = base[r] + wpre[ r * ncw + w ] + __popc( masks[ r * ncw + w ] & ( ( 1u << ( c & 31 ) ) - 1u ) );
+        inv[pos] = (uint16_t) i;
+    }
+    // permute each particle array in place through shared memory
+    uint32_t * arr[6] = { S.A.cell, reinterpret_cast<uint32_t *>( S.A.xx ), reinterpret_cast<uint32_t *>( S.A.xy ),
+                          reinterpret_cast<uint32_t *>( S.A.ux ), reinterpret_cast<uint32_t *>( S.A.uy ),
+                          reinterpret_cast<uint32_t *>( S.A.uz ) };
+    const int n4 = np >> 2;
+    for ( int a = 0; a < 6; a++ ) {
+        uint32_t * g = arr[a] + off;
+        __syncthreads();
+        for ( int v = threadIdx.x; v < n4; v += blockDim.x )
+            reinterpret_cast<uint4 *>( buf )[v] = reinterpret_cast<const uint4 *>( g )[v];
+        for ( int p = 4 * n4 + threadIdx.x; p < np; p += blockDim.x ) buf[p] = g[p];
+        __syncthreads();
+        for ( int v = threadIdx.x; v < n4; v += blockDim.x ) {
+            const int p = 4 * v;
+            reinterpret_cast<uint4 *>( g )[v] = make_uint4( buf[ inv[p] ], buf[ inv[p + 1] ], buf[ inv[p + 2] ], buf[ inv[p + 3] ] );
+        }
+        for ( int p = 4 * n4 + threadIdx.x; p < np; p += blockDim.x ) g[p] = buf[ inv[p] ];
+    }
+}
+
 }  // namespace zb
 
 // ---------------------------------------------------------------------------
@@ -1388,6 +1516,24 @@ cudaError_t launch_phasespace( cudaStream_t st, int sp, int ntiles, const SpDev 
 
 cudaError_t launch_energy_sum( cudaStream_t st, const SpDev * sps, int sp, int nitems, double * out ) {
     k_energy_sum<<< 1, 256, 0, st >>>( sps, sp, nitems, out );
+    return cudaGetLastError();
+}
+
+// Rounds (the most particles in one cell) and particles per tile that
+// k_reorder handles for tiles of up to max_cells cells, within 227 KB of
+// shared memory.
+cudaError_t launch_reorder( cudaStream_t st, const Item * items, int nitems, const SpDev * sps, const RunDev * runs,
+                            int max_cells ) {
+    if ( nitems <= 0 ) return cudaSuccess;
+    const int ncw = ( max_cells + 31 ) / 32;
+    const int rounds = std::max( 1, std::min( 511, ( 32 * 1024 ) / ( 6 * ncw ) - 1 ) );
+    const size_t fixed = (size_t) ncw * 32 * 4 + ( rounds + 1 ) * 4 + 16 + (size_t) rounds * ncw * 6;
+    const size_t budget = 227 * 1024;
+    if ( fixed + 64 * 6 > budget ) return cudaSuccess;
+    const int np_max = std::min<size_t>( 65532, ( ( budget - fixed ) / 6 ) & ~(size_t) 7 );
+    const size_t smem = (size_t) np_max * 6 + fixed;
+    cudaFuncSetAttribute( (const void *) k_reorder, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
+    k_reorder<<< nitems, RO_THREADS, smem, st >>>( items, sps, runs, rounds, np_max );
     return cudaGetLastError();
 }
 
