@@ -157,6 +157,12 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  *                         contributions rounded to 2^-29 |q| and summed exactly
  *                         in integer arithmetic, independent of the order of
  *                         the additions; the fastest of the three)
+ *   "reorder"        n    every n steps, put each tile's particles back into
+ *                         cell round-robin order (one particle of every cell,
+ *                         cells ascending, then the next round), which keeps
+ *                         the particle kernel's shared-memory bank conflicts at
+ *                         their initial level; 0 never (default).  Order only:
+ *                         every tile keeps its particle multiset.
  */
 int zpic_b200_sim_set_option( zpic_sim * sim, const char * key, double value );
 /* Autotuner (no reference counterpart): times `steps` steps for each

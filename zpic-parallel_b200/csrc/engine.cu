@@ -178,12 +178,23 @@ struct Plan {
     bool needs_bc_or_filter = false;
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
+    // in-graph phase timing (profile 2): the captured graph and its event-record
+    // nodes, pointed at fresh events before every replay
+    struct TimedPhase { int ph; int nl; cudaGraphNode_t na, nb; cudaEvent_t ea, eb; };
+    cudaGraph_t graph_src = nullptr;
+    std::vector<TimedPhase> timed;
     // moving-window steps, one graph per pattern of window moves
     std::map<unsigned, std::pair<cudaGraphExec_t, int>> mw_graphs;
     bool built = false;
 
-    void release() {
+    void drop_step_graph() {
         if ( graph ) { cudaGraphExecDestroy( graph ); graph = nullptr; }
+        if ( graph_src ) { cudaGraphDestroy( graph_src ); graph_src = nullptr; }
+        for ( auto & t : timed ) { cudaEventDestroy( t.ea ); cudaEventDestroy( t.eb ); }
+        timed.clear();
+    }
+    void release() {
+        drop_step_graph();
         for ( auto & g : mw_graphs ) cudaGraphExecDestroy( g.second.first );
         mw_graphs.clear();
         dfree( runs_d ); dfree( sps_d ); dfree( k1_items_d[0] ); dfree( k1_items_d[1] );
@@ -224,7 +235,7 @@ struct zpic_sim {
     int reorder_every = REORDER_DEFAULT;
     int chunks_opt = 0;
     int jacc = 2;                   // fixed-point tile current (option "jacc")
-    bool profile = false;
+    int profile = 0;                // 1: per-phase events, steps issued eagerly; 2: the same inside CUDA graphs
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[PH_N];
     double phase_ms[PH_N] = { 0 };
     uint64_t phase_launches[PH_N] = { 0 };
@@ -399,16 +410,38 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
 // ---------------------------------------------------------------------------
 // profiling helpers
 // ---------------------------------------------------------------------------
+// Phase events recorded while a step graph is captured for in-graph timing
+// (profile 2): they become event-record nodes, listed here with their phase.
+struct CapturedPhase { int ph; int nl; cudaEvent_t a, b; };
+static thread_local bool g_capture_timing = false;
+static thread_local std::vector<CapturedPhase> g_cap_events;
+
+// Inside a step graph only the particle phase is timed (two event nodes per
+// step: the nodes serialise with the kernels around them and cost about 1 us
+// each).
 struct PhaseScope {
-    zpic_sim * s; cudaStream_t st; int ph; cudaEvent_t a = nullptr, b = nullptr; int nl;
+    zpic_sim * s; cudaStream_t st; int ph; cudaEvent_t a = nullptr, b = nullptr; int nl; bool on = false;
     PhaseScope( zpic_sim * s_, cudaStream_t st_, int ph_, int nlaunch ) : s( s_ ), st( st_ ), ph( ph_ ), nl( nlaunch ) {
-        if ( s && s->profile ) { cudaEventCreate( &a ); cudaEventCreate( &b ); cudaEventRecord( a, st ); }
+        on = s && s->profile && ( !g_capture_timing || ph == PH_PARTICLES );
+        if ( on ) {
+            cudaEventCreate( &a ); cudaEventCreate( &b );
+            if ( g_capture_timing ) cudaEventRecordWithFlags( a, st, cudaEventRecordExternal );
+            else cudaEventRecord( a, st );
+        }
     }
     ~PhaseScope() {
         if ( !s ) return;
         s->launches += nl;
         s->phase_launches[ph] += nl;
-        if ( s->profile ) { cudaEventRecord( b, st ); s->ev_pending[ph].push_back( { a, b } ); }
+        if ( on ) {
+            if ( g_capture_timing ) {
+                cudaEventRecordWithFlags( b, st, cudaEventRecordExternal );
+                g_cap_events.push_back( { ph, nl, a, b } );
+            } else {
+                cudaEventRecord( b, st );
+                s->ev_pending[ph].push_back( { a, b } );
+            }
+        }
     }
 };
 
@@ -586,26 +619,78 @@ static int maybe_reorder( Plan & P, cudaStream_t st, uint64_t * launches ) {
 static int plan_advance( Plan & P, cudaStream_t st, int nsteps, bool use_graph, uint64_t * launches ) {
     for ( auto * s : P.sims ) TRY( ensure_jdep_clean( s, st ) );
     const bool can_graph = use_graph && nsteps > 1;
+    zpic_sim * ts = prof_sim( P );
+    const bool timing = ts && ts->profile == 2;
+    if ( can_graph && P.graph && timing != !P.timed.empty() ) P.drop_step_graph();
     if ( can_graph && !P.graph ) {
-        // Capture one step.  Launch counting and profiling are suspended
-        // during capture; replays count the graph's kernel nodes instead.
+        // Capture one step.  Launch counting is suspended during capture
+        // (replays count the graph's kernel nodes instead), and so is
+        // profiling unless the phases are to be timed inside the graph.
         std::vector<uint64_t> l0;
-        std::vector<char> prof;
-        for ( auto * s : P.sims ) { l0.push_back( s->launches ); prof.push_back( s->profile ); s->profile = false; }
+        std::vector<int> prof;
+        uint64_t pl0[PH_N] = { 0 };
+        if ( timing ) for ( int p = 0; p < PH_N; p++ ) pl0[p] = ts->phase_launches[p];
+        for ( auto * s : P.sims ) {
+            l0.push_back( s->launches ); prof.push_back( s->profile );
+            if ( !timing ) s->profile = 0;
+        }
+        g_capture_timing = timing;
+        g_cap_events.clear();
         cudaGraph_t g;
         CK( cudaStreamBeginCapture( st, cudaStreamCaptureModeThreadLocal ) );
         const int rc = plan_step_device( P, st );
         const cudaError_t e = cudaStreamEndCapture( st, &g );
+        g_capture_timing = false;
         for ( size_t i = 0; i < P.sims.size(); i++ ) { P.sims[i]->launches = l0[i]; P.sims[i]->profile = prof[i]; }
-        if ( rc != ZPIC_OK ) return rc;
-        if ( e != cudaSuccess ) return fail( ZPIC_E_CUDA, std::string( "graph capture: " ) + cudaGetErrorString( e ) );
+        if ( timing ) for ( int p = 0; p < PH_N; p++ ) ts->phase_launches[p] = pl0[p];
+        std::vector<CapturedPhase> cap;
+        cap.swap( g_cap_events );
+        if ( rc != ZPIC_OK || e != cudaSuccess ) {
+            for ( auto & c : cap ) { cudaEventDestroy( c.a ); cudaEventDestroy( c.b ); }
+            if ( rc != ZPIC_OK ) return rc;
+            return fail( ZPIC_E_CUDA, std::string( "graph capture: " ) + cudaGetErrorString( e ) );
+        }
         P.graph_kernels = count_graph_kernels( g );
+        if ( timing ) {
+            // event-record node of each captured phase event
+            size_t n = 0;
+            cudaGraphGetNodes( g, nullptr, &n );
+            std::vector<cudaGraphNode_t> nodes( n );
+            cudaGraphGetNodes( g, nodes.data(), &n );
+            std::map<cudaEvent_t, cudaGraphNode_t> node_of;
+            for ( auto & nd : nodes ) {
+                cudaGraphNodeType t;
+                cudaGraphNodeGetType( nd, &t );
+                cudaEvent_t ev;
+                if ( t == cudaGraphNodeTypeEventRecord && cudaGraphEventRecordNodeGetEvent( nd, &ev ) == cudaSuccess )
+                    node_of[ev] = nd;
+            }
+            for ( auto & c : cap ) {
+                auto ia = node_of.find( c.a ), ib = node_of.find( c.b );
+                if ( ia != node_of.end() && ib != node_of.end() )
+                    P.timed.push_back( { c.ph, c.nl, ia->second, ib->second, c.a, c.b } );
+                else { cudaEventDestroy( c.a ); cudaEventDestroy( c.b ); }
+            }
+        }
         const cudaError_t e2 = cudaGraphInstantiate( &P.graph, g, 0 );
-        cudaGraphDestroy( g );
-        if ( e2 != cudaSuccess ) { P.graph = nullptr; return fail( ZPIC_E_CUDA, std::string( "graph instantiate: " ) + cudaGetErrorString( e2 ) ); }
+        if ( timing ) P.graph_src = g;
+        else cudaGraphDestroy( g );
+        if ( e2 != cudaSuccess ) { P.graph = nullptr; P.drop_step_graph(); return fail( ZPIC_E_CUDA, std::string( "graph instantiate: " ) + cudaGetErrorString( e2 ) ); }
     }
     for ( int n = 0; n < nsteps; n++ ) {
         if ( can_graph && P.graph ) {
+            if ( timing ) {
+                // fresh events for this replay's phase nodes
+                for ( auto & t : P.timed ) {
+                    cudaEvent_t a, b;
+                    CK( cudaEventCreate( &a ) );
+                    CK( cudaEventCreate( &b ) );
+                    CK( cudaGraphExecEventRecordNodeSetEvent( P.graph, t.na, a ) );
+                    CK( cudaGraphExecEventRecordNodeSetEvent( P.graph, t.nb, b ) );
+                    ts->ev_pending[t.ph].push_back( { a, b } );
+                    ts->phase_launches[t.ph] += t.nl;
+                }
+            }
             CK( cudaGraphLaunch( P.graph, st ) );
             if ( launches ) *launches += P.graph_kernels;
         } else {
@@ -613,6 +698,14 @@ static int plan_advance( Plan & P, cudaStream_t st, int nsteps, bool use_graph, 
         }
         plan_step_host( P );
         TRY( maybe_reorder( P, st, launches ) );
+    }
+    if ( timing && P.graph ) {
+        // point the phase nodes back at the capture's own events, so that the
+        // replays' events can be destroyed once they have been read
+        for ( auto & t : P.timed ) {
+            CK( cudaGraphExecEventRecordNodeSetEvent( P.graph, t.na, t.ea ) );
+            CK( cudaGraphExecEventRecordNodeSetEvent( P.graph, t.nb, t.eb ) );
+        }
     }
     return ZPIC_OK;
 }
@@ -1078,7 +1171,15 @@ int zpic_b200_sim_set_option( zpic_sim * s, const char * key, double v ) {
     if ( !key ) return fail( ZPIC_E_INVALID, "null option" );
     std::string k( key );
     if ( k == "graph" ) { s->use_graph = v != 0; }
-    else if ( k == "profile" ) { s->profile = v != 0; if ( s->profile ) s->use_graph = false; }
+    else if ( k == "profile" ) {
+        // 1: events around each phase, steps issued eagerly; 2: events
+        // around the particle phase as nodes of the step graph, so that graph
+        // replays are timed
+        const int m = (int) v;
+        if ( m < 0 || m > 2 || m != v ) return fail( ZPIC_E_INVALID, "profile must be 0, 1 or 2" );
+        s->profile = m;
+        if ( m == 1 ) s->use_graph = false;
+    }
     else if ( k == "jacc" ) {
         const int j = (int) v;
         if ( j < 0 || j > 2 || j != v ) return fail( ZPIC_E_INVALID, "jacc must be 0, 1 or 2" );
@@ -1113,7 +1214,7 @@ int zpic_b200_sim_advance( zpic_sim * s, int32_t nsteps ) {
         }
     }
     uint64_t l = 0;
-    TRY( plan_advance( s->plan, s->stream, nsteps, s->use_graph && !s->profile, &l ) );
+    TRY( plan_advance( s->plan, s->stream, nsteps, s->use_graph && s->profile != 1, &l ) );
     s->launches += l;
     return ZPIC_OK;
 }
