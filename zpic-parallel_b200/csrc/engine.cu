@@ -32,7 +32,8 @@ cudaError_t launch_sort( cudaStream_t, const Item *, int, const SpDev *, const i
 cudaError_t launch_inject( cudaStream_t, int, int, int, int, int, const SpDev *, const RunDev *, const InjRule &, int );
 cudaError_t launch_inj_dyn( cudaStream_t, float *, unsigned *, int, float, float, float, double );
 cudaError_t launch_pack( cudaStream_t, int, int, const SpDev *, const int *, int2 *, float2 *, float * );
-cudaError_t launch_unpack( cudaStream_t, int, int, const SpDev *, const int *, const int2 *, const float2 *, const float * );
+cudaError_t launch_unpack( cudaStream_t, int, int, int, const SpDev *, const int *, long long, const int2 *, const float2 *,
+                           const float * );
 cudaError_t launch_gather( cudaStream_t, int, int, const SpDev *, const RunDev *, const int *, int, float, float, int, float * );
 cudaError_t launch_dep_charge( cudaStream_t, int, int, const SpDev *, const RunDev *, float *, int, int );
 cudaError_t launch_phasespace( cudaStream_t, int, int, const SpDev *, const RunDev *, PhaSpec, float * );
@@ -749,25 +750,81 @@ static int species_upload( zpic_sim * s, HSpecies * sp, const std::vector<int> &
     CK( cudaMemcpyAsync( sp->d.np, np.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
     CK( cudaMemcpyAsync( sp->d.off, off.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
     CK( cudaMemcpyAsync( sp->d.cap, cap.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
-    int * poff_d = nullptr; int2 * ix_d = nullptr; float2 * x_d = nullptr; float * u_d = nullptr;
+    int * poff_d = nullptr;
     TRY( dalloc( &poff_d, nt ) );
-    TRY( dalloc( &ix_d, total ) ); TRY( dalloc( &x_d, total ) ); TRY( dalloc( &u_d, 3 * total ) );
     CK( cudaMemcpyAsync( poff_d, poff.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
-    if ( total > 0 ) {
-        CK( cudaMemcpyAsync( ix_d, ix, total * sizeof( int2 ), cudaMemcpyHostToDevice, st ) );
-        CK( cudaMemcpyAsync( x_d, x, total * sizeof( float2 ), cudaMemcpyHostToDevice, st ) );
-        CK( cudaMemcpyAsync( u_d, u, total * 3 * sizeof( float ), cudaMemcpyHostToDevice, st ) );
-    }
     // the species descriptor must be on the device for the unpack kernel
     SpDev * one = nullptr;
     TRY( dalloc( &one, 1 ) );
     CK( cudaMemcpyAsync( one, &sp->d, sizeof( SpDev ), cudaMemcpyHostToDevice, st ) );
-    CK( launch_unpack( st, 0, nt, one, poff_d, ix_d, x_d, u_d ) );
-    s->launches++;
+    // Chunks of whole tiles staged in buffer B (free outside a step), two in
+    // flight: the host-to-device copies of one chunk, on a copy stream,
+    // overlap the unpack of the one before.  Even chunks use (B.cell, B.xx,
+    // B.ux), odd ones (B.xy, B.uy, B.uz); each array holds max_part 4-byte
+    // words, so a chunk holds up to max_part / 3 particles (12 bytes of
+    // momentum each).  A tile larger than that is staged in its own buffers.
+    const long long chunk_cap = std::max<long long>( 1, (long long) sp->max_part / 3 );
+    std::vector<int> cut( 1, 0 );
+    bool big = false;
+    {
+        long long acc = 0;
+        for ( int t = 0; t < nt; t++ ) {
+            if ( np[t] > chunk_cap ) big = true;
+            if ( acc + np[t] > chunk_cap && t > cut.back() ) { cut.push_back( t ); acc = 0; }
+            acc += np[t];
+        }
+        cut.push_back( nt );
+    }
+    std::vector<int2 *> own_ix; std::vector<float2 *> own_x; std::vector<float *> own_u;
+    cudaStream_t cs = nullptr;
+    cudaEvent_t copied[2] = { nullptr, nullptr }, unpacked[2] = { nullptr, nullptr };
+    CK( cudaStreamCreateWithFlags( &cs, cudaStreamNonBlocking ) );
+    for ( int b = 0; b < 2; b++ ) {
+        CK( cudaEventCreateWithFlags( &copied[b], cudaEventDisableTiming ) );
+        CK( cudaEventCreateWithFlags( &unpacked[b], cudaEventDisableTiming ) );
+    }
+    // the copy stream starts after the work already on the simulation's stream
+    CK( cudaEventRecord( unpacked[0], st ) );
+    CK( cudaStreamWaitEvent( cs, unpacked[0], 0 ) );
+    int rc = ZPIC_OK;
+    for ( size_t k = 0; k + 1 < cut.size() && rc == ZPIC_OK; k++ ) {
+        const int t0 = cut[k], t1 = cut[k + 1], b = (int) ( k & 1 );
+        const long long p0 = poff[t0], n = ( t1 < nt ? (long long) poff[t1] : total ) - p0;
+        int2 * ix_d; float2 * x_d; float * u_d;
+        if ( big ) {
+            int2 * a = nullptr; float2 * c = nullptr; float * e = nullptr;
+            if ( ( rc = dalloc( &a, n ) ) != ZPIC_OK || ( rc = dalloc( &c, n ) ) != ZPIC_OK || ( rc = dalloc( &e, 3 * n ) ) != ZPIC_OK ) {
+                dfree( a ); dfree( c ); dfree( e );
+                break;
+            }
+            own_ix.push_back( a ); own_x.push_back( c ); own_u.push_back( e );
+            ix_d = a; x_d = c; u_d = e;
+        } else {
+            ix_d = reinterpret_cast<int2 *>( b ? (void *) sp->d.B.xy : (void *) sp->d.B.cell );
+            x_d = reinterpret_cast<float2 *>( b ? sp->d.B.uy : sp->d.B.xx );
+            u_d = b ? sp->d.B.uz : sp->d.B.ux;
+            if ( k >= 2 ) CK( cudaStreamWaitEvent( cs, unpacked[b], 0 ) );
+        }
+        if ( n > 0 ) {
+            CK( cudaMemcpyAsync( ix_d, ix + 2 * p0, n * sizeof( int2 ), cudaMemcpyHostToDevice, cs ) );
+            CK( cudaMemcpyAsync( x_d, x + 2 * p0, n * sizeof( float2 ), cudaMemcpyHostToDevice, cs ) );
+            CK( cudaMemcpyAsync( u_d, u + 3 * p0, n * 3 * sizeof( float ), cudaMemcpyHostToDevice, cs ) );
+        }
+        CK( cudaEventRecord( copied[b], cs ) );
+        CK( cudaStreamWaitEvent( st, copied[b], 0 ) );
+        CK( launch_unpack( st, 0, t0, t1 - t0, one, poff_d, p0, ix_d, x_d, u_d ) );
+        s->launches++;
+        CK( cudaEventRecord( unpacked[b], st ) );
+    }
+    CK( cudaStreamSynchronize( st ) );
+    for ( int b = 0; b < 2; b++ ) { cudaEventDestroy( copied[b] ); cudaEventDestroy( unpacked[b] ); }
+    cudaStreamDestroy( cs );
+    for ( size_t i = 0; i < own_ix.size(); i++ ) { dfree( own_ix[i] ); dfree( own_x[i] ); dfree( own_u[i] ); }
+    if ( rc != ZPIC_OK ) { dfree( one ); dfree( poff_d ); return rc; }
     CK( cudaMemsetAsync( sp->d.in_cnt, 0, nt * sizeof( int ), st ) );
     CK( cudaMemsetAsync( sp->d.nidx, 0, nt * sizeof( int ), st ) );
     CK( cudaStreamSynchronize( st ) );
-    dfree( one ); dfree( poff_d ); dfree( ix_d ); dfree( x_d ); dfree( u_d );
+    dfree( one ); dfree( poff_d );
     sp->np_bound = total;
     sp->sort_pending = false;
     sp->counters_dirty = false;

@@ -1090,12 +1090,13 @@ __global__ void k_pack( int sp, const SpDev * __restrict__ sps, const int * __re
     }
 }
 
-__global__ void k_unpack( int sp, const SpDev * __restrict__ sps, const int * __restrict__ poff,
+__global__ void k_unpack( int sp, const SpDev * __restrict__ sps, const int * __restrict__ poff, int t0, long long pbase,
                           const int2 * __restrict__ ix, const float2 * __restrict__ x, const float * __restrict__ u )
 {
     const SpDev & S = sps[sp];
-    const int t = blockIdx.x;
-    const int np = S.np[t], off = S.off[t], po = poff[t];
+    const int t = t0 + blockIdx.x;
+    const int np = S.np[t], off = S.off[t];
+    const long long po = poff[t] - pbase;
     for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
         const size_t g = (size_t) off + i, s = (size_t) po + i;
         S.A.cell[g] = pack_cell( ix[s].x, ix[s].y );
@@ -1483,9 +1484,12 @@ cudaError_t launch_pack( cudaStream_t st, int sp, int ntiles, const SpDev * sps,
     return cudaGetLastError();
 }
 
-cudaError_t launch_unpack( cudaStream_t st, int sp, int ntiles, const SpDev * sps, const int * poff,
-                           const int2 * ix, const float2 * x, const float * u ) {
-    k_unpack<<< ntiles, 256, 0, st >>>( sp, sps, poff, ix, x, u );
+// Tiles [t0, t0 + ntiles) from packed arrays holding the particles from
+// packed offset pbase on.
+cudaError_t launch_unpack( cudaStream_t st, int sp, int t0, int ntiles, const SpDev * sps, const int * poff,
+                           long long pbase, const int2 * ix, const float2 * x, const float * u ) {
+    if ( ntiles <= 0 ) return cudaSuccess;
+    k_unpack<<< ntiles, 256, 0, st >>>( sp, sps, poff, t0, pbase, ix, x, u );
     return cudaGetLastError();
 }
 
