@@ -45,6 +45,9 @@ UNIT = 'pushes/s'
 # particle kernel also reads E and B (24 B/cell) and writes J (12 B/cell)
 BYTES_PER_PUSH = 56
 PARTICLE_KERNEL_BYTES_PER_CELL = 36
+# the whole step's algorithmic bytes per cell: the particle kernel's 36 plus
+# the Yee solve (read E, B, J: 36 B; write E, B: 24 B)
+STEP_BYTES_PER_CELL = 96
 
 
 def workload_config(ncell=NCELL):
@@ -338,6 +341,12 @@ def run_gpu(args, world, rank, local):
             'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded Thermal uth 0.05)',
             'config': workload_config(ncell),
             'roofline': roofline,
+            'step_roofline': {
+                'bytes_per_step': BYTES_PER_PUSH * np_total + STEP_BYTES_PER_CELL * ncell * ncell,
+                'achieved': (BYTES_PER_PUSH * np_total + STEP_BYTES_PER_CELL * ncell * ncell) / (t_max / args.steps / 1e3) / 1e9,
+                'unit': 'GB/s',
+                'frac': (BYTES_PER_PUSH * np_total + STEP_BYTES_PER_CELL * ncell * ncell) / (t_max / args.steps / 1e3) / 1e9 / hbm,
+                'note': 'whole step (56 B per particle push + 96 B per cell) over the timed step time'},
             'cpu_baseline': cpu,
             'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d / args.steps,
                     'd2h_bytes_per_step': d2h,
