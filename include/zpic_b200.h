@@ -150,7 +150,10 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  *   "chunks"         n    CTAs per tile in the particle kernel: n > 0 for every
  *                         tile, 0 automatic (default), -1 automatic and in
  *                         proportion to each tile's particles
- *   "profile"        1/0  record CUDA events around each kernel phase
+ *   "profile"        0/1/2 phase timing read by zpic_b200_sim_phase_times: 1
+ *                         CUDA events around each kernel phase, steps issued
+ *                         without a graph; 2 events around the particle kernel
+ *                         as nodes of the step graph (graph replays timed)
  *   "jacc"           0/1/2 tile current accumulation in shared memory: 0 FP32
  *                         atomics (the reference's FP32 sums, in another order),
  *                         1 FP64 atomics, 2 fixed point (default: the FP32
