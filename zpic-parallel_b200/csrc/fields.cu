@@ -261,7 +261,8 @@ k_yee( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, in
         float4 * z = reinterpret_cast<float4 *>( R.Jdep + toff );
         for ( int i = threadIdx.x; i < 3 * tv / 4; i += blockDim.x ) z[i] = make_float4( 0.f, 0.f, 0.f, 0.f );
     }
-    if ( threadIdx.x == 0 ) bulk_wait_all();
+    // the shared-memory sources read; the stores complete before the kernel does
+    if ( threadIdx.x == 0 ) bulk_wait_read_all();
 }
 
 // ---------------------------------------------------------------------------

@@ -593,7 +593,9 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
             fence_proxy_async_smem();
             bulk_s2g_add_f32( R.Jdep + (size_t) t * 3 * tv, sJout, 12u * tv );
             bulk_commit();
-            bulk_wait_all();
+            // the CTA may leave once its shared memory has been read; the
+            // global additions complete before the kernel does
+            bulk_wait_read_all();
         }
     }
 }
