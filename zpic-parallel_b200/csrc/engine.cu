@@ -227,6 +227,8 @@ struct zpic_sim {
     RunDev run{};
     int * status = nullptr;
     double * dscratch = nullptr;   // small device scratch (energies, stats)
+    double * fe_part_d = nullptr;  // per-tile field-energy partials (6 per tile), device
+    double * fe_part_h = nullptr;  // and their pinned host copy, allocated on first use
     double * hscratch = nullptr;   // pinned host mirror
     int * shifts_d = nullptr;
     std::vector<HSpecies *> species;
@@ -1129,7 +1131,8 @@ int zpic_b200_sim_destroy( zpic_sim * s ) {
     s->plan.release();
     for ( auto * sp : s->species ) { sp->free_all(); delete sp; }
     dfree( s->run.E ); dfree( s->run.B ); dfree( s->run.J ); dfree( s->run.Jdep );
-    dfree( s->status ); dfree( s->dscratch ); dfree( s->shifts_d );
+    dfree( s->status ); dfree( s->dscratch ); dfree( s->shifts_d ); dfree( s->fe_part_d );
+    if ( s->fe_part_h ) { cudaFreeHost( s->fe_part_h ); s->fe_part_h = nullptr; }
     if ( s->hscratch ) cudaFreeHost( s->hscratch );
     cudaStreamDestroy( s->stream );
     delete s;
@@ -1427,14 +1430,18 @@ int zpic_b200_emf_energy( zpic_sim * s, double ene_E[3], double ene_B[3] ) {
     TRY( sim_select( s ) );
     TRY( ensure_plan( s ) );
     const int nt = s->ntx * s->nty;
-    double * part = nullptr;
-    TRY( dalloc( &part, 6 * (size_t) nt ) );
-    CK( launch_field_energy( s->stream, s->plan.runs_d, 0, nt, part ) );
+    // partials buffers kept for the simulation's lifetime (a per-step
+    // diagnostic: no allocation, no pageable copy per call)
+    if ( !s->fe_part_d ) TRY( dalloc( &s->fe_part_d, 6 * (size_t) nt ) );
+    if ( !s->fe_part_h ) {
+        const cudaError_t e = cudaMallocHost( (void **) &s->fe_part_h, 6 * (size_t) nt * sizeof( double ) );
+        if ( e != cudaSuccess ) { s->fe_part_h = nullptr; return fail( ZPIC_E_NOMEM, std::string( "cudaMallocHost: " ) + cudaGetErrorString( e ) ); }
+    }
+    CK( launch_field_energy( s->stream, s->plan.runs_d, 0, nt, s->fe_part_d ) );
     s->launches++;
-    std::vector<double> h( 6 * (size_t) nt );
-    CK( cudaMemcpyAsync( h.data(), part, h.size() * sizeof( double ), cudaMemcpyDeviceToHost, s->stream ) );
+    const double * h = s->fe_part_h;
+    CK( cudaMemcpyAsync( s->fe_part_h, s->fe_part_d, 6 * (size_t) nt * sizeof( double ), cudaMemcpyDeviceToHost, s->stream ) );
     CK( cudaStreamSynchronize( s->stream ) );
-    dfree( part );
     double e[6] = { 0, 0, 0, 0, 0, 0 };
     for ( int t = 0; t < nt; t++ ) for ( int k = 0; k < 6; k++ ) e[k] += h[6 * (size_t) t + k];   // tile order
     for ( int k = 0; k < 3; k++ ) { ene_E[k] = e[k]; ene_B[k] = e[3 + k]; }
