@@ -493,25 +493,39 @@ k_shift_left( const TileItem * __restrict__ items, const RunDev * __restrict__ r
     }
 }
 
-// EMF::get_energy (emf.cpp:662-713): per tile, six sequential FP64 sums in
-// the reference's loop order (note its inner bound nx.y); one lane each.
-__global__ void k_field_energy( const RunDev * __restrict__ runs, int run, double * __restrict__ out )
+// EMF::get_energy (emf.cpp:662-713): per tile, six FP64 sums of the FP32
+// squares over the reference's loop range (note its inner bound nx.y).
+__global__ void k_field_energy( const RunDev * __restrict__ runs, int run, double * __restrict__ out, int ntiles )
 {
     const RunDev & R = runs[run];
-    const int t = blockIdx.x;
-    const int k = threadIdx.x;
-    if ( k >= 6 ) return;
-    const float * g = ( k < 3 ? R.E : R.B ) + ( (size_t) t * R.tile_vol + R.gc_off ) * 3 + ( k % 3 );
-    double s = 0.0;
+    const int lane = threadIdx.x & 31;
+    const int t = blockIdx.x * ( blockDim.x >> 5 ) + ( threadIdx.x >> 5 );      // a warp per tile
+    if ( t >= ntiles ) return;
     // inner bound nx.y as in the reference; limited to the tile row (ext_x - 1
     // cells from x = 0) where nx.y exceeds it
     const int ixmax = min( R.nxy, R.extx - GL );
-    for ( int iy = 0; iy < R.nxy; iy++ )
-        for ( int ix = 0; ix < ixmax; ix++ ) {
-            const float v = g[ 3 * ( iy * R.extx + ix ) ];
-            s += v * v;
+    const int ncell = R.nxy * ixmax;
+    const float * e = R.E + ( (size_t) t * R.tile_vol + R.gc_off ) * 3;
+    const float * b = R.B + ( (size_t) t * R.tile_vol + R.gc_off ) * 3;
+    // each term v * v in FP32, summed in FP64 (emf.cpp:662-713); lanes take
+    // every 32nd cell, then a fixed-order warp tree
+    double s[6] = { 0.0, 0.0, 0.0, 0.0, 0.0, 0.0 };
+    for ( int c = lane; c < ncell; c += 32 ) {
+        const int iy = c / ixmax, ix = c - iy * ixmax;
+        const int o = 3 * ( iy * R.extx + ix );
+#pragma unroll
+        for ( int k = 0; k < 3; k++ ) {
+            const float v = e[ o + k ], w = b[ o + k ];
+            s[k] += v * v;
+            s[3 + k] += w * w;
         }
-    out[ 6 * t + k ] = s;
+    }
+#pragma unroll
+    for ( int k = 0; k < 6; k++ ) {
+#pragma unroll
+        for ( int d = 16; d > 0; d >>= 1 ) s[k] += __shfl_down_sync( 0xffffffffu, s[k], d );
+        if ( lane == 0 ) out[ 6 * t + k ] = s[k];
+    }
 }
 
 // Adds a tiled grid: dst += src over whole tile blocks (Laser::Pulse::add, laser.h:85-99)
@@ -612,7 +626,7 @@ cudaError_t launch_shift_left( cudaStream_t st, const TileItem * items, int n, c
     return cudaGetLastError();
 }
 cudaError_t launch_field_energy( cudaStream_t st, const RunDev * runs, int run, int ntiles, double * out ) {
-    k_field_energy<<< ntiles, 32, 0, st >>>( runs, run, out );
+    k_field_energy<<< ( ntiles + 7 ) / 8, 256, 0, st >>>( runs, run, out, ntiles );
     return cudaGetLastError();
 }
 cudaError_t launch_grid_add( cudaStream_t st, float * dst, const float * src, size_t n ) {
