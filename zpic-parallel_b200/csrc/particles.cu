@@ -279,7 +279,10 @@ __device__ __forceinline__ int wrap_tile( int v, int n, int periodic ) {
 
 constexpr int PK_THREADS = 256;
 constexpr int PK_PPT = 2;                   // particles per thread per block iteration
-constexpr int FLUSH_PARTICLES = 16384;      // particles between fixed-point flushes
+// Particles between fixed-point flushes: at most 3 additions per particle and
+// accumulator pair, 61,440 < 2^16 per group.  Tiles of 16x16 cells at 8x8
+// particles per cell (16,384 on average) then run without a flush.
+constexpr int FLUSH_PARTICLES = 20480;
 static_assert( FLUSH_PARTICLES % ( PK_PPT * PK_THREADS ) == 0, "flush groups hold whole blocks" );
 
 // Adds the fixed-point tile current accumulated so far (hi words at acc[0, n),
