@@ -146,7 +146,7 @@ def test_move_deposit_fixed_point_tile_current():
 
 def test_fixed_point_flush_dense_tiles():
     """65,536 particles per tile in one CTA: the fixed-point tile current is
-    flushed to the raw current between groups of 16,384 particles; the
+    flushed to the raw current between groups of 20,480 particles; the
     deposited current stays within the FP32 bar of the oracle's."""
     geom = ((2, 2), (16, 16), (3.2, 3.2), 0.07)
 
