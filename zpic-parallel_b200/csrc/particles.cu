@@ -750,8 +750,9 @@ k_sort_out( const Item * __restrict__ items, int nitems, const SpDev * __restric
     const int tib = warp / WPT, sub = warp % WPT;
     const unsigned lt = ( 1u << lane ) - 1u;
     __shared__ int s_nh[TPB], s_ns[TPB];
-    if ( threadIdx.x < TPB ) { s_nh[threadIdx.x] = 0; s_ns[threadIdx.x] = 0; }
-    __syncthreads();
+    // one tile per warp (WPT 1): the warp's own counters, warp-level syncs
+    if ( sub == 0 && lane == 0 ) { s_nh[tib] = 0; s_ns[tib] = 0; }
+    if ( WPT > 1 ) __syncthreads(); else __syncwarp();
 
     const int wi = blockIdx.x * TPB + tib;
     bool active = wi < nitems;
@@ -829,7 +830,7 @@ k_sort_out( const Item * __restrict__ items, int nitems, const SpDev * __restric
             }
         }
     }
-    __syncthreads();
+    if ( WPT > 1 ) __syncthreads(); else __syncwarp();
     if ( active ) {
         const SpDev & S = *Sp;
         const int nh = s_nh[tib], ns = s_ns[tib], nh2 = min( nh, ns );
