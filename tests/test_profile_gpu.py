@@ -45,3 +45,17 @@ def test_profile_modes(mode):
     b.synchronize()
     with pytest.raises(zb.ZpicError):
         b.set_option('profile', 3)
+
+
+def test_profile_graph_mode_moving_window():
+    """Moving-window steps are issued eagerly when profiled (mode 2 included)
+    and time every phase."""
+    s = zb.Simulation((16, 4), (16, 16), (256 * 0.025, 64 * 0.1), 0.022)
+    s.add_species(-1.0, (4, 2), density=('step', 1.0, 2.0, 0))
+    s.set_moving_window()
+    s.set_option('profile', 2)
+    s.advance_mov_window(5)
+    s.synchronize()
+    ph = s.phase_times()
+    assert ph['particles'][1] == 5 and ph['particles'][0] > 0
+    assert ph['fields'][1] > 0

@@ -84,3 +84,19 @@ def test_reorder_moving_window():
     ea, eb = a.emf_energy(), b.emf_energy()
     assert rel_err(eb[0].sum(), ea[0].sum()) <= 1e-4
     assert rel_err(b.species_energy(0), a.species_energy(0)) <= 1e-4
+
+
+def test_reorder_skips_tiles_beyond_shared_memory():
+    """32x32 tiles holding 65,536 particles each do not fit the reorder's
+    shared-memory permutation: they keep their order, and nothing changes."""
+    geom = ((2, 2), (32, 32), (6.4, 6.4), 0.07)
+
+    def dense(s):
+        s.add_species(-1.0, (8, 8), udist=('thermal', (0.05, 0.05, 0.05), (0, 0, 0)))
+        return s
+    a, b = dense(zb.Simulation(*geom)), dense(zb.Simulation(*geom))
+    b.set_option('reorder', 1)
+    a.advance(1)
+    b.advance(1)
+    assert same_multisets(a.particles(0), b.particles(0))
+    assert b.np_total(0) == 64 * 64 * 64
