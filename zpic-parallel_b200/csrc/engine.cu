@@ -194,8 +194,17 @@ struct Plan {
         for ( auto & t : timed ) { cudaEventDestroy( t.ea ); cudaEventDestroy( t.eb ); }
         timed.clear();
     }
+    // a second stream for the field half of a step: after the particle
+    // kernel, the tile sort (particle arrays only) and the current and field
+    // solve (grids only) are independent and run side by side
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+
     void release() {
         drop_step_graph();
+        if ( fork ) { cudaEventDestroy( fork ); fork = nullptr; }
+        if ( join ) { cudaEventDestroy( join ); join = nullptr; }
+        if ( side ) { cudaStreamDestroy( side ); side = nullptr; }
         for ( auto & g : mw_graphs ) cudaGraphExecDestroy( g.second.first );
         mw_graphs.clear();
         dfree( runs_d ); dfree( sps_d ); dfree( k1_items_d[0] ); dfree( k1_items_d[1] );
@@ -388,6 +397,9 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
     TRY( dalloc( &P.splist_d, splist.size() ) );
     TRY( dalloc( &P.tile_items_d, tiles.size() ) );
     TRY( dalloc( &P.sort_items_d, sort_items.size() ) );
+    CK( cudaStreamCreateWithFlags( &P.side, cudaStreamNonBlocking ) );
+    CK( cudaEventCreateWithFlags( &P.fork, cudaEventDisableTiming ) );
+    CK( cudaEventCreateWithFlags( &P.join, cudaEventDisableTiming ) );
     CK( cudaMemcpy( P.runs_d, runs.data(), runs.size() * sizeof( RunDev ), cudaMemcpyHostToDevice ) );
     if ( !P.sps_h.empty() ) {
         CK( cudaMemcpy( P.sps_d, P.sps_h.data(), P.sps_h.size() * sizeof( SpDev ), cudaMemcpyHostToDevice ) );
@@ -578,9 +590,15 @@ static int ensure_jdep_clean( zpic_sim * s, cudaStream_t st ) {
 // One Simulation::advance (simulation.h:90-107) for all sims of a plan, on st.
 static int plan_step_device( Plan & P, cudaStream_t st ) {
     TRY( run_particles( P, st, 1, 2, nullptr ) );
+    // the sort on the simulation's stream, current and fields on the side
+    // stream (forked after the particle kernel, joined before the step ends)
+    DEV( cudaEventRecord( P.fork, st ) );
+    DEV( cudaStreamWaitEvent( P.side, P.fork, 0 ) );
+    TRY( run_current( P, P.side ) );
+    TRY( run_fields( P, P.side, 1, 0, 1 ) );
+    DEV( cudaEventRecord( P.join, P.side ) );
     TRY( run_sort( P, st, 0 ) );
-    TRY( run_current( P, st ) );
-    TRY( run_fields( P, st, 1, 0, 1 ) );
+    DEV( cudaStreamWaitEvent( st, P.join, 0 ) );
     return ZPIC_OK;
 }
 
