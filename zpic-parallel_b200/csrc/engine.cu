@@ -976,12 +976,21 @@ static int species_sort( zpic_sim * s, int sp, int use_extra ) {
 }
 
 // Species::advance_mov_window (species.cpp:2083-2128) for one species
-static int species_advance_mw( zpic_sim * s, int sp ) {
+// The particle kernel of a moving-window species step; *moving tells
+// whether this step shifts the species' window (then the kernel shifts the
+// particles by one cell).
+static int mw_species_kernel( zpic_sim * s, int sp, bool * moving ) {
     HSpecies * h = s->species[sp];
     TRY( ensure_plan( s ) );
     const float t = ( h->iter + 1 ) * h->dt;        // int * float, as in the reference
-    if ( h->mw.needs_move( t ) ) {
-        TRY( species_kernel( s, sp, 1, 2, s->shifts_d ) );
+    *moving = h->mw.needs_move( t );
+    return species_kernel( s, sp, 1, 2, *moving ? s->shifts_d : nullptr );
+}
+
+// The rest of it: injection of the new column when the window moves, tile sort.
+static int mw_species_finish( zpic_sim * s, int sp, bool moving ) {
+    HSpecies * h = s->species[sp];
+    if ( moving ) {
         const unsigned gx = s->ntx * s->nxx, gy = s->nty * s->nxy;
         const unsigned range[4] = { gx - 1, gx - 1, 0, gy - 1 };
         InjRule r = inj_rule( s, h, range );
@@ -1016,11 +1025,16 @@ static int species_advance_mw( zpic_sim * s, int sp ) {
         }
         h->mw.advance();
     } else {
-        TRY( species_kernel( s, sp, 1, 2, nullptr ) );
         TRY( species_sort( s, sp, 0 ) );
     }
     h->iter++;
     return ZPIC_OK;
+}
+
+static int species_advance_mw( zpic_sim * s, int sp ) {
+    bool moving = false;
+    TRY( mw_species_kernel( s, sp, &moving ) );
+    return mw_species_finish( s, sp, moving );
 }
 
 // ---- autotuning of CTAs per tile ----
@@ -1298,22 +1312,38 @@ int zpic_b200_sim_advance( zpic_sim * s, int32_t nsteps ) {
 }
 
 // One Simulation::advance_mov_window step (simulation.h:113-130): species,
-// current, fields and the window shift, issued on the simulation's stream.
+// current, fields and the window shift.  After the particle kernels the
+// species' injection and sort (particle arrays only) stay on the
+// simulation's stream while current, fields and the field shift (grids only)
+// run on the plan's side stream; the two join before the step ends.
 static int mw_step( zpic_sim * s ) {
     TRY( ensure_jdep_clean( s, s->stream ) );
+    TRY( ensure_plan( s ) );
     s->j_final = false;
-    for ( size_t k = 0; k < s->species.size(); k++ ) TRY( species_advance_mw( s, (int) k ) );
-    TRY( run_current( s->plan, s->stream ) );
+    const size_t nsp = s->species.size();
+    std::vector<char> moving( nsp, 0 );
+    for ( size_t k = 0; k < nsp; k++ ) {
+        bool m = false;
+        TRY( mw_species_kernel( s, (int) k, &m ) );
+        moving[k] = m;
+    }
+    Plan & P = s->plan;
+    DEV( cudaEventRecord( P.fork, s->stream ) );
+    DEV( cudaStreamWaitEvent( P.side, P.fork, 0 ) );
+    TRY( run_current( P, P.side ) );
     s->cur_iter++;
     if ( s->cur_mw.needs_move( s->cur_iter * s->dt ) ) s->cur_mw.advance();
-    TRY( run_fields( s->plan, s->stream, 1, 0, 1 ) );
+    TRY( run_fields( P, P.side, 1, 0, 1 ) );
     s->jdep_clean = true;
     s->j_final = true;
     s->emf_iter++;
     if ( s->emf_mw.active && s->emf_mw.needs_move( s->emf_iter * s->dt ) ) {
-        TRY( run_shift( s->plan, s->stream, 0 ) );
+        TRY( run_shift( P, P.side, 0 ) );
         s->emf_mw.advance();
     }
+    DEV( cudaEventRecord( P.join, P.side ) );
+    for ( size_t k = 0; k < nsp; k++ ) TRY( mw_species_finish( s, (int) k, moving[k] != 0 ) );
+    DEV( cudaStreamWaitEvent( s->stream, P.join, 0 ) );
     s->iter++;
     return ZPIC_OK;
 }
