@@ -292,7 +292,8 @@ def run_gpu(args, world, rank, local):
         'launch_ms': per_launch_ms,
         'phase_ms_per_step': {k: v[0] / args.steps for k, v in ph.items()},
         'phase_note': 'launch_ms: particle kernel timed by event nodes of the step graph during the timed steps; '
-                      'phase_ms_per_step: the K steps after them, issued eagerly with events around every phase',
+                      'phase_ms_per_step: the K steps after them, issued eagerly with events around every phase '
+                      '(the sort and the current + field phases run side by side on two streams)',
     }
 
     # ---- end-to-end through the C-ABI with host buffers ----
