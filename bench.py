@@ -78,12 +78,17 @@ def ncu_traffic_per_particle():
 
 
 class ClockSampler:
-    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed
+    region: the sampler is started and its first sample awaited before the
+    region begins, and only samples that arrive inside it are kept (the one
+    nearest to it when the region is shorter than the sampling period)."""
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=25):
         self.index = index
+        self.period_ms = period_ms
         self.proc = None
-        self.lines = []
+        self.lines = []                       # (arrival time, csv line)
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -92,20 +97,26 @@ class ClockSampler:
                  '--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
                  'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
                  'clocks_event_reasons.sw_power_cap',
-                 '--format=csv,noheader,nounits', '-lms', '200'],
+                 '--format=csv,noheader,nounits', '-lms', str(self.period_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.perf_counter() + 2.0
+            while not self.lines and time.perf_counter() < deadline and self.proc.poll() is None:
+                time.sleep(0.005)
         except (OSError, FileNotFoundError):
             self.proc = None
+        self.t0 = time.perf_counter()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
     def __exit__(self, *a):
+        self.t1 = time.perf_counter()
         if self.proc:
+            time.sleep(2 * self.period_ms / 1e3)      # the samples still in the pipe
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -113,9 +124,13 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        slack = 2 * self.period_ms / 1e3
+        inside = [ln for ts, ln in self.lines if self.t0 is not None and self.t0 <= ts <= self.t1 + slack]
+        if not inside and self.lines and self.t0 is not None:
+            inside = [min(self.lines, key=lambda e: abs(e[0] - self.t0))[1]]
         sm, mx, reasons = [], None, set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        for ln in self.lines:
+        for ln in inside:
             f = [x.strip() for x in ln.split(',')]
             if len(f) < 7:
                 continue
