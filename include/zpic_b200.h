@@ -183,7 +183,10 @@ int zpic_b200_sim_phase_times( zpic_sim * sim, double * ms, uint64_t * launches,
 int zpic_b200_sim_reset_phase_times( zpic_sim * sim );
 /* Kernel launches issued by the library for this handle since creation. */
 int zpic_b200_sim_launch_count( zpic_sim * sim, uint64_t * count );
-/* The cudaStream_t all work of this handle runs on (for external event timing). */
+/* The cudaStream_t of this handle (for external event timing).  Every call's
+ * work is ordered on it: a step also runs part of its kernels on a second,
+ * internal stream, forked from this one and joined back into it before the
+ * step ends, so events recorded on it bracket whole calls. */
 int zpic_b200_sim_stream( zpic_sim * sim, void ** stream );
 
 /* ---- EMF (emf.h:24-197) ---- */
