@@ -336,6 +336,29 @@ def run_gpu(args, world, rank, local):
     # species energy (1 double) + per-tile field energy partials (6 doubles per
     # tile, summed on the host in tile order as EMF::get_energy does)
     d2h = 8 + 6 * 8 * (ncell // TILE) ** 2
+    sim.close()
+
+    # ---- chosen vs plain: the same workload and timing with the plain FP32
+    # tile current (FP32 shared-memory atomics, the reference's FP32 sums in
+    # another order; option jacc 0) ----
+    psim = make_sim(zb, ncell, local, args)
+    psim.set_option('jacc', 0)
+    pstream = torch.cuda.ExternalStream(psim.stream_handle(), device=local)
+    psim.advance(args.warmup)
+    psim.synchronize()
+    pn0 = psim.nmove()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    q0.record(pstream)
+    psim.advance(args.steps)
+    q1.record(pstream)
+    q1.synchronize()
+    tp = max_over_ranks(q0.elapsed_time(q1), world)
+    plain = {'value': (psim.nmove() - pn0) * world / (tp / 1e3), 'unit': UNIT, 'ms_per_step': tp / args.steps,
+             'how': 'same steps with FP32 shared-memory atomics for the tile current (option jacc 0) '
+                    'instead of the fixed-point accumulation'}
+    psim.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -374,9 +397,10 @@ def run_gpu(args, world, rank, local):
             'gpu_launches': launches,
             'clocks': clocks,
             'cell_updates_per_second': ncell * ncell * args.steps * world / (t_max / 1e3),
+            'plain': plain,
+            'chosen_over_plain': value / plain['value'],
         }
         print(json.dumps(line))
-    sim.close()
     return 0
 
 
