@@ -265,10 +265,13 @@ __device__ __noinline__ void drain_entry( const CrossQueue & Q, int e, float qnx
 // 512-particle block (2 per thread keeps 4 CTAs per SM resident without
 // spills, 35% faster than 4 per thread): every access is a fully coalesced 128 B
 // warp transaction, and consecutive lanes (consecutive particles, which the
-// injection order puts in consecutive cells) hit distinct shared-memory banks.
-// Particles that stay in their cell deposit one segment at once; particles
-// that cross a cell edge are queued per warp and split/deposited in full-warp
-// passes, so the two- and three-segment code runs without divergence.
+// injection order puts in consecutive cells) spread over the shared-memory
+// banks (about 2-way conflicts; as particles drift between the cells of their
+// tile the order decays towards random cells, about 3.5-way, which the
+// optional in-tile reorder undoes).  Particles that stay in their cell deposit
+// one segment at once; particles that cross a cell edge are queued per warp
+// and split/deposited in full-warp passes, so the split runs on full warps
+// (only a third segment, for the rare double crossings, diverges).
 // ---------------------------------------------------------------------------
 // Target tile index along one axis for a particle leaving through v (periodic
 // wrap, or -1 past an open edge).
