@@ -249,20 +249,27 @@ int zpic_b200_grid_gather( zpic_sim * sim, int32_t which, int32_t fc, float * ou
  * ---- charge density without device allocation ----
  * No counterpart in the reference.  Same result as zpic_b200_species_charge
  * (dense [ny][nx] charge density of one particle set), for callers that
- * cannot allocate device memory: frameworks that own all device memory
- * through their own pool, allocation-free real-time / in-situ loops, and
- * code recorded into CUDA graphs (cudaMalloc cannot be captured).
+ * cannot allocate device memory: a host framework that owns all device
+ * memory through its own pool and forbids foreign allocations, or a
+ * real-time or in-situ analysis loop inside another code's time step that
+ * must not stall on the allocator (cudaMalloc may synchronise the device).
  * The caller passes device pointers: per-tile particle counts and offsets of
  * a packed particle set (the layout zpic_b200_species_get returns: ix as
  * 2 int32, x as 2 float per particle), the charge per particle q, and the
  * output grid of ntiles_x*nx_x * ntiles_y*nx_y floats; work is queued on
  * `stream` (a cudaStream_t, or NULL for the default stream).
+ * Precondition: every particle's cell lies inside its tile,
+ * 0 <= ix.x < nx_x and 0 <= ix.y < nx_y (a sorted set, as species_get returns
+ * it); particles outside are skipped, not deposited.
  * Scratch lives in a fixed 32 MiB device array owned by the library (held on
- * every GPU that loads it until exit): ntiles * roundup4((nx_x+1)*(nx_y+1))
- * must not exceed 8 Mi floats, larger grids are rejected with ZPIC_E_INVALID.
- * The first call on a device resolves the array's address on that device;
- * make that first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU race and must be serialised.
+ * every GPU that loads it until exit).  Limits, checked before any work is
+ * queued (ZPIC_E_INVALID otherwise): a tile block of (nx_x+1)*(nx_y+1) cells
+ * at most 12288, and ntiles_x*ntiles_y * roundup4((nx_x+1)*(nx_y+1)) at most
+ * 8 Mi floats.  The first call on a device (and the first after that
+ * device's context was reset) resolves the array's address on that device;
+ * make that first call before any stream capture.  All calls share the
+ * array, which keeps the last call's contents (each call clears the part it
+ * uses): calls that overlap on the GPU race and must be serialised.
  */
 int zpic_b200_charge_deposit_noalloc( uint32_t ntiles_x, uint32_t ntiles_y, uint32_t nx_x, uint32_t nx_y,
                                       float q, const int32_t * np, const int32_t * offset,

@@ -1,9 +1,10 @@
 """zpic_b200_charge_deposit_noalloc: the charge density for callers that cannot
-allocate device memory (frameworks owning all device memory, allocation-free
-real-time loops, work recorded into CUDA graphs).  The caller allocates the
-inputs and the output; the entry point itself uses the library's fixed
-scratch array and must give the same density as zpic_b200_species_charge,
-call after call (the shared scratch is cleared by each call).
+allocate device memory (a framework that owns all device memory through its
+own pool, a real-time or in-situ loop that must not stall on the allocator).
+The caller allocates the inputs and the output; the entry point itself uses
+the library's fixed scratch array and must give the same density as
+zpic_b200_species_charge, call after call (the shared scratch is cleared by
+each call).
 
 This file is collected last so that a run stopping at the first failure has
 run every other test before it.
@@ -29,9 +30,9 @@ def _weibel():
     return sim
 
 
-def _noalloc_charge(sim, sp):
+def _noalloc_charge(sim, sp, parts=None):
     import torch
-    npt, ix, x, _ = sim.particles(sp)
+    npt, ix, x, _ = parts if parts is not None else sim.particles(sp)
     off = np.zeros_like(npt)
     off[1:] = np.cumsum(npt)[:-1]
     d_np = torch.from_numpy(npt).cuda()
@@ -63,3 +64,35 @@ def test_noalloc_rejects_grid_beyond_scratch():
     with pytest.raises(zb.ZpicError, match='maximum'):
         zb.charge_deposit_noalloc((512, 512), (16, 16), 1.0, dummy.data_ptr(), dummy.data_ptr(),
                                   dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr(), 0)
+
+
+def test_noalloc_rejects_oversized_tiles_before_any_work():
+    """Tile sides whose guard-cell block would overflow 32-bit arithmetic
+    (65535 + 1 squared wraps to 0) are rejected on the host, like any tile
+    block above 12,288 cells."""
+    import torch
+    dummy = torch.zeros(4, dtype=torch.int32, device='cuda')
+    for nx in ((65535, 65535), (12288, 1), (110, 110), (4294967295, 1)):
+        with pytest.raises(zb.ZpicError, match='maximum'):
+            zb.charge_deposit_noalloc((1, 1), nx, 1.0, dummy.data_ptr(), dummy.data_ptr(),
+                                      dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr(), 0)
+
+
+def test_noalloc_skips_particles_outside_their_tile():
+    """Particles whose cell lies outside their tile (an unsorted set) are
+    skipped: the result is the deposit of the others."""
+    sim = _weibel()
+    npt, ix, x, u = sim.particles(0)
+    bad = ix.copy()
+    bad[0] = (-1, 0)
+    bad[1] = (GEOM[1][0], 3)
+    bad[2] = (5, GEOM[1][1] + 7)
+    got = _noalloc_charge(sim, 0, (npt, bad, x, u))
+    keep = np.ones(len(ix), bool)
+    keep[:3] = False
+    # the same set with those three particles removed (they sit in tile 0)
+    npt2 = npt.copy()
+    npt2[0] -= 3
+    ref = _noalloc_charge(sim, 0, (npt2, ix[keep], x[keep], u[keep]))
+    assert np.isfinite(got).all()
+    assert np.abs(got - ref).max() <= RHO_TOL * np.abs(ref).max()
