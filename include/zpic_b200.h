@@ -166,6 +166,14 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  *                         the particle kernel's shared-memory bank conflicts at
  *                         their initial level; 0 never (default).  Order only:
  *                         every tile keeps its particle multiset.
+ *   "capacity_factor" f   initial particle capacity of species added after
+ *                         this call: f * cells * ppc (default 1.2, the
+ *                         reference's max_part, species.cpp:1752); buffers grow
+ *                         when injection or species_set needs more
+ *   "wait_limit"     n    polls before a kernel's bounded wait on its bulk
+ *                         copies gives up (default 4194304, ~0.5 s); a kernel
+ *                         that gives up skips its work for that tile and the
+ *                         next synchronising call returns ZPIC_E_DEVICE
  */
 int zpic_b200_sim_set_option( zpic_sim * sim, const char * key, double value );
 /* Autotuner (no reference counterpart): times `steps` steps for each
@@ -217,6 +225,10 @@ int zpic_b200_species_np_total( zpic_sim * sim, int32_t sp, uint64_t * np );   /
  * copy of its particles through the second buffer); no reference counterpart. */
 int zpic_b200_species_repacks( zpic_sim * sim, int32_t sp, uint64_t * repacks );
 int zpic_b200_species_np_max_tile( zpic_sim * sim, int32_t sp, uint32_t * np );/* Species::np_max_tile */
+/* Particle-buffer capacity (the public Particles::max_part, particles.h:82-105).
+ * It grows, as the reference's does in its sort (particles.cpp:863-888), when
+ * injection or species_set needs more room. */
+int zpic_b200_species_max_part( zpic_sim * sim, int32_t sp, uint32_t * max_part );
 /* Tile information in the reference's packed layout: offset[t] = sum of np before t (particles.h:94-97) */
 int zpic_b200_species_get_tiles( zpic_sim * sim, int32_t sp, int32_t * np, int32_t * offset );
 /* Particle data in the reference's packed layout (ix: 2 int32, x: 2 float, u: 3 float per particle) */

@@ -128,6 +128,7 @@ struct HSpecies {
     int ntiles = 0;
     uint32_t max_part = 0;
     uint64_t np_bound = 0;    // upper bound of the particle count (capacity checks)
+    int grows = 0;            // particle-buffer growths so far
     SpDev d{};                // descriptor (device pointers)
     bool sort_pending = false;
     bool counters_dirty = false;
@@ -247,11 +248,14 @@ struct zpic_sim {
     int reorder_every = REORDER_DEFAULT;
     int chunks_opt = 0;
     int jacc = 2;                   // fixed-point tile current (option "jacc")
+    double capacity_factor = 1.2;   // initial particle capacity per cell and ppc (option "capacity_factor";
+                                    // the reference's max_part = 1.2 cells ppc, species.cpp:1752)
     int profile = 0;                // 1: per-phase events, steps issued eagerly; 2: the same inside CUDA graphs
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[PH_N];
     double phase_ms[PH_N] = { 0 };
     uint64_t phase_launches[PH_N] = { 0 };
     uint64_t launches = 0;
+    uint64_t layout_gen = 0;        // bumped when device buffers or descriptors change (batch plans rebuild)
 
     int tile_vol() const { return run.tile_vol; }
     size_t grid_floats() const { return (size_t) run.tile_vol * ntx * nty * 3; }
@@ -264,6 +268,7 @@ struct zpic_batch {
     cudaEvent_t ev = nullptr;
     uint64_t launches = 0;          // kernels launched by batch steps
     int chunks = 0;                 // CTAs per tile chosen for the batch (0 = automatic)
+    std::vector<uint64_t> gens;     // layout_gen of each run when the plan was built
 };
 
 static int sim_select( zpic_sim * s ) {
@@ -272,11 +277,16 @@ static int sim_select( zpic_sim * s ) {
     return ZPIC_OK;
 }
 
+// Reads the kernels' status word.  A failure is reported once: the word is
+// cleared when it is read, so a later call starts clean (the state the
+// failed work left behind is not repaired).
 static int check_status( zpic_sim * s ) {
     int st = 0;
     CK( cudaMemcpyAsync( &st, s->status, sizeof( int ), cudaMemcpyDeviceToHost, s->stream ) );
     CK( cudaStreamSynchronize( s->stream ) );
     if ( st & ( ST_WAIT_TIMEOUT | ST_CAPACITY | ST_BAD_CELL ) ) {
+        CK( cudaMemsetAsync( s->status, 0, sizeof( int ), s->stream ) );
+        CK( cudaStreamSynchronize( s->stream ) );
         std::string m = "device reported:";
         if ( st & ST_WAIT_TIMEOUT ) m += " bounded wait expired;";
         if ( st & ST_CAPACITY ) m += " particle buffer capacity exceeded;";
@@ -323,6 +333,7 @@ static int upload_run( zpic_sim * s ) {
     R.cur_perx = s->cur_bc[0] == ZPIC_CURRENT_BC_PERIODIC; R.cur_pery = s->cur_bc[2] == ZPIC_CURRENT_BC_PERIODIC;
     for ( int k = 0; k < 4; k++ ) { R.emf_bc[k] = s->emf_bc[k]; R.cur_bc[k] = s->cur_bc[k]; }
     s->plan.built = false;
+    s->layout_gen++;
     return ZPIC_OK;
 }
 
@@ -877,6 +888,81 @@ static int species_alloc( zpic_sim * s, HSpecies * sp, uint64_t max_part ) {
     return ZPIC_OK;
 }
 
+// Capacity a species needs for `total` particles: after a sort every tile's
+// slot is rounded up to 4 particles, so up to 3 more per tile.
+static uint64_t capacity_for( const HSpecies * h, uint64_t total ) { return total + 4ull * h->ntiles; }
+
+// Particle-buffer growth (Particles::grow_buffer, particles.h:174-190: the
+// reference grows its buffers in multiples of 64 Ki particles when a sort's
+// new total exceeds max_part, particles.cpp:863-888).  New arrays of new_max
+// particles; the live contents are copied -- the tile slots of A, and the
+// leaver outbox (B) and leaver lists (idx) that a pending sort still reads --
+// the new room lies after the last slot (the next repack spreads it over the
+// tiles).  The plans' device copies of the descriptor are rewritten in
+// place, so that step graphs already captured (their kernels read the
+// descriptor from device memory) run on the new buffers.
+static int species_grow( zpic_sim * s, HSpecies * h, uint64_t new_max ) {
+    new_max = ( new_max + 65535 ) & ~(uint64_t) 65535;
+    if ( new_max <= h->max_part ) return ZPIC_OK;
+    if ( new_max > (uint64_t) INT32_MAX ) return fail( ZPIC_E_NOMEM, "particle buffer would exceed 2^31 particles" );
+    CK( cudaStreamSynchronize( s->stream ) );
+    if ( s->plan.built && s->plan.side ) CK( cudaStreamSynchronize( s->plan.side ) );
+    SpDev & d = h->d;
+    const size_t old = h->max_part;
+    const int stage_cap = (int) std::max<uint64_t>( 65536, new_max / 4 );
+    PartArrays A{}, B{}, S{};
+    int * idx = nullptr; int * aux = nullptr; int * aux2 = nullptr;
+    int rc = alloc_arrays( A, new_max );
+    if ( rc == ZPIC_OK ) rc = alloc_arrays( B, new_max );
+    if ( rc == ZPIC_OK ) rc = alloc_arrays( S, stage_cap );
+    if ( rc == ZPIC_OK ) rc = dalloc( &idx, new_max );
+    if ( rc == ZPIC_OK ) rc = dalloc( &aux, new_max );
+    if ( rc == ZPIC_OK ) rc = dalloc( &aux2, new_max );
+    if ( rc != ZPIC_OK ) {
+        PartArrays * na[3] = { &A, &B, &S };
+        for ( auto * a : na ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
+        dfree( idx ); dfree( aux ); dfree( aux2 );
+        return rc;
+    }
+    const size_t w = old * sizeof( float );
+    PartArrays * src[2] = { &d.A, &d.B }, * dst[2] = { &A, &B };
+    for ( int k = 0; k < 2; k++ ) {
+        CK( cudaMemcpyAsync( dst[k]->cell, src[k]->cell, w, cudaMemcpyDeviceToDevice, s->stream ) );
+        CK( cudaMemcpyAsync( dst[k]->xx, src[k]->xx, w, cudaMemcpyDeviceToDevice, s->stream ) );
+        CK( cudaMemcpyAsync( dst[k]->xy, src[k]->xy, w, cudaMemcpyDeviceToDevice, s->stream ) );
+        CK( cudaMemcpyAsync( dst[k]->ux, src[k]->ux, w, cudaMemcpyDeviceToDevice, s->stream ) );
+        CK( cudaMemcpyAsync( dst[k]->uy, src[k]->uy, w, cudaMemcpyDeviceToDevice, s->stream ) );
+        CK( cudaMemcpyAsync( dst[k]->uz, src[k]->uz, w, cudaMemcpyDeviceToDevice, s->stream ) );
+    }
+    CK( cudaMemcpyAsync( idx, d.idx, old * sizeof( int ), cudaMemcpyDeviceToDevice, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    PartArrays * olds[3] = { &d.A, &d.B, &d.S };
+    for ( auto * a : olds ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
+    dfree( d.idx ); dfree( d.aux ); dfree( d.aux2 );
+    d.A = A; d.B = B; d.S = S; d.idx = idx; d.aux = aux; d.aux2 = aux2;
+    d.max_part = (int) new_max;
+    d.stage_cap = stage_cap;
+    h->max_part = (uint32_t) new_max;
+    h->grows++;
+    // the descriptor copies of this simulation's plan
+    Plan & P = s->plan;
+    if ( P.built ) {
+        for ( size_t i = 0; i < P.sps_h.size(); i++ ) {
+            if ( P.sp_local[i] >= 0 && P.sp_local[i] < (int) s->species.size() && s->species[ P.sp_local[i] ] == h ) {
+                SpDev v = d;
+                v.run = P.sps_h[i].run;
+                v.nchunk = P.sps_h[i].nchunk;
+                v.chunk_target = P.sps_h[i].chunk_target;
+                P.sps_h[i] = v;
+                CK( cudaMemcpyAsync( P.sps_d + i, &P.sps_h[i], sizeof( SpDev ), cudaMemcpyHostToDevice, s->stream ) );
+            }
+        }
+        CK( cudaStreamSynchronize( s->stream ) );
+    }
+    s->layout_gen++;
+    return ZPIC_OK;
+}
+
 static void species_params( zpic_sim * s, HSpecies * sp ) {
     SpDev & d = sp->d;
     d.alpha = 0.5 * sp->dt / sp->m_q;                  // species.cpp:2305
@@ -998,14 +1084,18 @@ static int mw_species_finish( zpic_sim * s, int sp, bool moving ) {
         // column of cells is injected per move
         const uint64_t add = h->dens.type == ZPIC_DENSITY_NONE ? 0 : (uint64_t) gy * h->ppc[0] * h->ppc[1];
         h->np_bound += add;
-        if ( h->np_bound > h->max_part ) {
+        if ( capacity_for( h, h->np_bound ) > h->max_part ) {
             // the bound is loose once particles leave; read the real count
             unsigned long long st2[2];
             DEV( launch_np_stats( s->stream, s->plan.sps_d, sp, (unsigned long long *) s->dscratch ) );
             CK( cudaMemcpyAsync( st2, s->dscratch, sizeof( st2 ), cudaMemcpyDeviceToHost, s->stream ) );
             CK( cudaStreamSynchronize( s->stream ) );
             h->np_bound = st2[0] + add;
-            if ( h->np_bound > h->max_part ) return fail( ZPIC_E_NOMEM, "particle buffer too small for the moving-window injection" );
+            // still short: grow (by a quarter at least, so that a steadily
+            // injecting run grows rarely)
+            if ( capacity_for( h, h->np_bound ) > h->max_part )
+                TRY( species_grow( s, h, std::max<uint64_t>( capacity_for( h, h->np_bound ),
+                                                             (uint64_t) h->max_part + h->max_part / 4 ) ) );
         }
         if ( h->dens.type != ZPIC_DENSITY_NONE ) {
             // the window-dependent rule parameters come from the device's move count
@@ -1141,6 +1231,7 @@ int zpic_b200_sim_create( uint32_t ntx, uint32_t nty, uint32_t nxx, uint32_t nxy
     TRY( dalloc( &s->status, 1 ) );
     CK( cudaMemset( s->status, 0, sizeof( int ) ) );
     R.status = s->status;
+    R.wait_limit = WAIT_LIMIT_DEFAULT;
     TRY( dalloc( &s->dscratch, 64 ) );
     CK( cudaMallocHost( (void **) &s->hscratch, 64 * sizeof( double ) ) );
     // cell shift of a moving-window step: -1 for whichever species the
@@ -1204,7 +1295,7 @@ int zpic_b200_sim_add_species( zpic_sim * s, const zpic_species_desc * desc, int
     sp->q = std::copysign( n0, sp->m_q ) / ( sp->ppc[0] * sp->ppc[1] );
     const float dimsx = (float) ( s->nxx * s->ntx ), dimsy = (float) ( s->nxy * s->nty );
     sp->dx[0] = sp->box[0] / dimsx; sp->dx[1] = sp->box[1] / dimsy;
-    const uint64_t ref_max = (uint64_t) ( 1.2 * dimsx * dimsy * sp->ppc[0] * sp->ppc[1] );
+    const uint64_t ref_max = (uint64_t) ( s->capacity_factor * dimsx * dimsy * sp->ppc[0] * sp->ppc[1] );
     const int nt = s->ntx * s->nty;
     // initial particles on the host, reference algorithms and order
     zbhost::Injector I = injector( s, sp.get() );
@@ -1282,6 +1373,20 @@ int zpic_b200_sim_set_option( zpic_sim * s, const char * key, double v ) {
         if ( r < 0 || r != v ) return fail( ZPIC_E_INVALID, "reorder must be a step count >= 0" );
         s->reorder_every = r;
         s->plan.release();
+    }
+    else if ( k == "capacity_factor" ) {
+        // initial particle-buffer capacity of species added afterwards, in
+        // particles per cell per ppc (buffers grow when they run short)
+        if ( !( v > 0 && v <= 64 ) ) return fail( ZPIC_E_INVALID, "capacity_factor must be in (0, 64]" );
+        s->capacity_factor = v;
+    }
+    else if ( k == "wait_limit" ) {
+        // polls of the kernels' bounded waits on their bulk copies before
+        // they give up (default ~0.5 s worth)
+        const int w = (int) v;
+        if ( w < 1 || w != v ) return fail( ZPIC_E_INVALID, "wait_limit must be a poll count >= 1" );
+        s->run.wait_limit = w;
+        TRY( upload_run( s ) );
     }
     else if ( k == "chunks" ) {
         // the per-item energy array holds 64 chunks per tile
@@ -1368,7 +1473,7 @@ int zpic_b200_sim_advance_mov_window( zpic_sim * s, int32_t nsteps ) {
             if ( h->mw.needs_move( (float) ( ( h->iter + 1 ) * h->dt ) ) ) {
                 key |= 1u << k;
                 const uint64_t add = h->dens.type == ZPIC_DENSITY_NONE ? 0 : (uint64_t) gy * h->ppc[0] * h->ppc[1];
-                if ( h->np_bound + add > h->max_part ) eager = true;
+                if ( capacity_for( h, h->np_bound + add ) > h->max_part ) eager = true;
             }
         }
         if ( s->emf_mw.active && s->emf_mw.needs_move( ( s->emf_iter + 1 ) * s->dt ) ) key |= 1u << 31;
@@ -1649,6 +1754,13 @@ int zpic_b200_species_repacks( zpic_sim * s, int32_t sp, uint64_t * repacks ) {
     return ZPIC_OK;
 }
 
+int zpic_b200_species_max_part( zpic_sim * s, int32_t sp, uint32_t * max_part ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    if ( !max_part ) return fail( ZPIC_E_INVALID, "null argument" );
+    *max_part = s->species[sp]->max_part;
+    return ZPIC_OK;
+}
+
 int zpic_b200_sim_nmove( zpic_sim * s, uint64_t * nmove ) {
     TRY( sim_select( s ) );
     uint64_t t = 0;
@@ -1724,8 +1836,14 @@ int zpic_b200_species_set( zpic_sim * s, int32_t sp, const int32_t * np, const i
     TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
     HSpecies * h = s->species[sp];
     std::vector<int> n( np, np + h->ntiles );
-    for ( int v : n ) if ( v < 0 ) return fail( ZPIC_E_INVALID, "negative particle count" );
+    uint64_t need = 0;
+    for ( int v : n ) {
+        if ( v < 0 ) return fail( ZPIC_E_INVALID, "negative particle count" );
+        need += roundup4( v );
+    }
     CK( cudaStreamSynchronize( s->stream ) );
+    // a set larger than the buffer grows it (with a fifth to spare)
+    if ( need + 4ull * h->ntiles > h->max_part ) TRY( species_grow( s, h, ( need + 4ull * h->ntiles ) * 6 / 5 ) );
     TRY( species_upload( s, h, n, ix, x, u ) );
     return ZPIC_OK;
 }
@@ -1887,13 +2005,29 @@ int zpic_b200_batch_create( zpic_sim * const * sims, int32_t n, zpic_batch ** ou
     CK( cudaStreamCreateWithFlags( &b->stream, cudaStreamNonBlocking ) );
     CK( cudaEventCreateWithFlags( &b->ev, cudaEventDisableTiming ) );
     TRY( plan_build( b->plan, b->sims, b->chunks ) );
+    for ( auto * s : b->sims ) b->gens.push_back( s->layout_gen );
     *out = b.release();
+    return ZPIC_OK;
+}
+
+// A run whose buffers or descriptors changed since the batch's plan was built
+// (options, boundaries, particle-buffer growth) makes the batch rebuild it.
+static int batch_refresh( zpic_batch * b ) {
+    bool stale = b->gens.size() != b->sims.size();
+    for ( size_t i = 0; i < b->sims.size() && !stale; i++ ) stale = b->gens[i] != b->sims[i]->layout_gen;
+    if ( !stale ) return ZPIC_OK;
+    for ( auto * s : b->sims ) CK( cudaStreamSynchronize( s->stream ) );
+    CK( cudaStreamSynchronize( b->stream ) );
+    TRY( plan_build( b->plan, b->sims, b->chunks ) );
+    b->gens.clear();
+    for ( auto * s : b->sims ) b->gens.push_back( s->layout_gen );
     return ZPIC_OK;
 }
 
 int zpic_b200_batch_advance( zpic_batch * b, int32_t nsteps ) {
     if ( !b ) return fail( ZPIC_E_INVALID, "null batch" );
     CK( cudaSetDevice( b->sims[0]->device ) );
+    TRY( batch_refresh( b ) );
     for ( auto * s : b->sims ) {
         if ( !s->plan.built ) TRY( ensure_plan( s ) );
         CK( cudaEventRecord( b->ev, s->stream ) );

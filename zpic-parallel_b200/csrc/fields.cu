@@ -238,8 +238,8 @@ k_yee( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, in
         bulk_g2s( sB, R.B + toff, bytes, bar );
         if ( with_j ) bulk_g2s( sJ, Jsrc + toff, bytes, bar );
     }
-    mbar_wait_bounded( bar, 0, R.status );
-    __syncthreads();
+    // an expired wait: no field update and no stores for this tile
+    if ( bulk_wait_or_abandon( bar, R.status, R.wait_limit ) ) return;
 
     float * E0 = sE + 3 * R.gc_off;
     float * B0 = sB + 3 * R.gc_off;

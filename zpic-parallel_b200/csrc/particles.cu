@@ -367,8 +367,16 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     if ( MOVE == 2 ) {
         for ( int i = threadIdx.x; i < 3 * tv * JW; i += blockDim.x ) sJ[i] = (JT) 0;
     }
-    if ( PUSH ) mbar_wait_bounded( bar, 0, R.status );
-    __syncthreads();
+    if ( PUSH ) {
+        // an expired wait: the item's particles, current and energy are left
+        // as they were (the step is reported failed)
+        if ( bulk_wait_or_abandon( bar, R.status, R.wait_limit ) ) {
+            if ( threadIdx.x == 0 ) S.energy[ eidx ] = 0.0;
+            return;
+        }
+    } else {
+        __syncthreads();
+    }
 
     const int ys = TN ? TN + 3 : R.extx;
     const int gc_off = TN ? TN + 4 : R.gc_off;

@@ -39,6 +39,7 @@ struct RunDev {
     int emf_bc[4];                // emf::bc
     int cur_bc[4];                // current::bc
     int * status;                 // ST_* bits
+    int wait_limit;               // polls of a bounded wait before it gives up (option "wait_limit")
 };
 
 // Particle arrays of one buffer (A, repack buffer B or staging).
@@ -148,15 +149,33 @@ __device__ __forceinline__ void bulk_wait_all() {
     asm volatile( "cp.async.bulk.wait_group 0;" ::: "memory" );
 }
 
-// Bounded wait on an mbarrier phase.  Gives up after ~0.5 s, records
-// ST_WAIT_TIMEOUT and returns false; never traps.
-__device__ __forceinline__ bool mbar_wait_bounded( uint64_t * bar, uint32_t parity, int * status ) {
-    for ( int i = 0; i < ( 1 << 22 ); i++ ) {
+// Polls of a bounded wait by default: ~0.5 s.
+constexpr int WAIT_LIMIT_DEFAULT = 1 << 22;
+
+// Bounded wait on an mbarrier phase.  Gives up after `limit` polls, records
+// ST_WAIT_TIMEOUT (when status is given) and returns false; never traps.
+__device__ __forceinline__ bool mbar_wait_bounded( uint64_t * bar, uint32_t parity, int * status,
+                                                   int limit = WAIT_LIMIT_DEFAULT ) {
+    for ( int i = 0; i < limit; i++ ) {
         if ( mbar_try_wait_parity( bar, parity ) ) return true;
         if ( i > 16 ) __nanosleep( 128 );
     }
-    atomicOr( status, ST_WAIT_TIMEOUT );
+    if ( status ) atomicOr( status, ST_WAIT_TIMEOUT );
     return false;
+}
+
+// Bulk copies into shared memory complete on an mbarrier.  A CTA whose wait
+// gave up must not compute on (or store) what has not arrived, and must not
+// exit while its copies may still write its shared memory: every thread
+// learns whether any thread gave up, and if so waits once more, with the
+// default limit, for the copies to land.  Returns true when the CTA must
+// skip its work and return.
+__device__ __forceinline__ bool bulk_wait_or_abandon( uint64_t * bar, int * status, int limit ) {
+    const bool ok = mbar_wait_bounded( bar, 0, status, limit );
+    if ( !__syncthreads_or( !ok ) ) return false;
+    mbar_wait_bounded( bar, 0, status, WAIT_LIMIT_DEFAULT );
+    __syncthreads();
+    return true;
 }
 
 // Tile-local cell index packing

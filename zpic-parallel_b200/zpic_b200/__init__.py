@@ -48,6 +48,7 @@ EXPORTS = [
     'zpic_b200_species_move', 'zpic_b200_species_process_bc', 'zpic_b200_species_tile_sort',
     'zpic_b200_species_set_bc', 'zpic_b200_species_set_push_type', 'zpic_b200_species_energy',
     'zpic_b200_species_nmove', 'zpic_b200_species_np_total', 'zpic_b200_species_np_max_tile',
+    'zpic_b200_species_max_part',
     'zpic_b200_species_get_tiles', 'zpic_b200_species_get', 'zpic_b200_species_set',
     'zpic_b200_species_gather', 'zpic_b200_species_charge', 'zpic_b200_species_phasespace',
     'zpic_b200_grid_size', 'zpic_b200_grid_get', 'zpic_b200_grid_set', 'zpic_b200_grid_gather',
@@ -141,6 +142,7 @@ def lib():
             'zpic_b200_species_nmove': (I, [P, I, U64P]),
             'zpic_b200_species_np_total': (I, [P, I, U64P]),
             'zpic_b200_species_np_max_tile': (I, [P, I, ctypes.POINTER(U)]),
+            'zpic_b200_species_max_part': (I, [P, I, ctypes.POINTER(U)]),
             'zpic_b200_species_get_tiles': (I, [P, I, IP, IP]),
             'zpic_b200_species_get': (I, [P, I, IP, FP, FP]),
             'zpic_b200_species_set': (I, [P, I, IP, IP, FP, FP]),
@@ -361,6 +363,12 @@ class Simulation:
     def np_max_tile(self, sp):
         v = ctypes.c_uint32()
         _check(lib().zpic_b200_species_np_max_tile(self.h, sp, ctypes.byref(v)))
+        return v.value
+
+    def max_part(self, sp):
+        """Particle-buffer capacity of species sp (Particles::max_part; grows on demand)."""
+        v = ctypes.c_uint32()
+        _check(lib().zpic_b200_species_max_part(self.h, sp, ctypes.byref(v)))
         return v.value
 
     def emf_energy(self):
