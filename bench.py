@@ -48,6 +48,11 @@ PARTICLE_KERNEL_BYTES_PER_CELL = 36
 # the whole step's algorithmic bytes per cell: the particle kernel's 36 plus
 # the Yee solve (read E, B, J: 36 B; write E, B: 24 B)
 STEP_BYTES_PER_CELL = 96
+# steady-state timing starts after this many steps of the run
+STEADY_AFTER = 100
+# the batched Weibel ensemble: runs and steps of the workload
+ENSEMBLE_RUNS = 256
+ENSEMBLE_STEPS = 500
 
 
 def workload_config(ncell=NCELL):
@@ -206,11 +211,11 @@ def run_reference(args, world, rank):
     if not ref_available('scalar') and not ref_available('avx2'):
         print(json.dumps({'impl': 'reference', 'unavailable': 'reference build oracle/_ref missing'}))
         return 0
-    # bounded sample of the workload: same tiles, ppc and temperature on a
-    # smaller box, so that the run finishes within a few minutes
-    ncell = args.ref_cells
+    # the workload itself (2048^2 cells, 268 M particles: ~8 GB of host
+    # memory, ~0.4 s per step on 16 cores) unless a smaller box is asked for
+    ncell = args.reference_cells
     rate, tstep, cores, variant = reference_sample(ncell, args.steps, args.warmup)
-    cfg = workload_config(NCELL)
+    cfg = workload_config(ncell)
     line = {
         'metric': METRIC, 'value': rate, 'unit': UNIT, 'impl': 'reference',
         'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
@@ -218,9 +223,10 @@ def run_reference(args, world, rank):
         'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded)',
         'config': cfg,
         'cpu_baseline': {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'reference',
-                         'sample': '%dx%d cells of the workload (%d particles), openmp/em2d %s build, '
-                                   '%d threads, step loop timed' % (ncell, ncell, ncell * ncell * PPC * PPC,
-                                                                    variant, cores)},
+                         'sample': '%dx%d cells (%d particles), openmp/em2d %s build, %d threads, '
+                                   '%d steps after %d untimed, step loop timed'
+                                   % (ncell, ncell, ncell * ncell * PPC * PPC, variant, cores,
+                                      args.steps, args.warmup)},
         'e2e': {'value': rate, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
     print(json.dumps(line))
@@ -291,12 +297,32 @@ def run_gpu(args, world, rank, local):
     sim.advance(args.steps)
     sim.synchronize()
     ph = sim.phase_times()
+    # ---- steady state: the same timing once the run is past 100 steps (the
+    # particles' in-tile order has decayed, as in the workload's 100-step runs) ----
+    sim.set_option('profile', 2)
+    done = args.warmup + 2 * args.steps
+    sim.advance(max(0, STEADY_AFTER - done))
+    sim.synchronize()
+    sim.reset_phase_times()
+    s0, m0 = sim.iter(), sim.nmove()
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    w0.record(stream)
+    sim.advance(args.steps)
+    w1.record(stream)
+    w1.synchronize()
+    ts = max_over_ranks(w0.elapsed_time(w1), world)
+    sp_ms, sp_n = sim.phase_times()['particles']
+    steady = {'after_steps': s0, 'steps': args.steps, 'ms_per_step': ts / args.steps,
+              'value': (sim.nmove() - m0) * world / (ts / 1e3), 'unit': UNIT,
+              'particle_launch_ms': sp_ms / max(1, sp_n)}
     sim.set_option('profile', 0)
     sim.set_option('graph', 1)
     per_launch_ms = part_ms / max(1, part_n)
     hbm, peak_kind = peaks()
     alg_bytes = BYTES_PER_PUSH * np_total + PARTICLE_KERNEL_BYTES_PER_CELL * ncell * ncell
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    steady['roofline_frac'] = alg_bytes / (steady['particle_launch_ms'] / 1e3) / 1e9 / hbm
     tpp = ncu_traffic_per_particle()
     roofline = {
         'kernel': 'k_particles (fused push, move, deposit, walls, leaver detection)',
@@ -374,6 +400,12 @@ def run_gpu(args, world, rank, local):
         except Exception as e:  # reported, not fatal
             cpu = {'value': None, 'error': str(e)}
 
+    # ---- the ensemble half of the metric: batched vs plain run-steps/s on
+    # the 256-run Weibel ensemble, its own 500 steps whatever --steps says ----
+    ens = None
+    if not args.no_ensemble:
+        ens = ensemble_measure(args, world, rank, local, ENSEMBLE_RUNS, ENSEMBLE_STEPS)
+
     clocks = clk.summary()
     if rank == 0:
         line = {
@@ -399,7 +431,10 @@ def run_gpu(args, world, rank, local):
             'cell_updates_per_second': ncell * ncell * args.steps * world / (t_max / 1e3),
             'plain': plain,
             'chosen_over_plain': value / plain['value'],
+            'steady_state': steady,
         }
+        if ens is not None:
+            line['ensemble'] = ens
         print(json.dumps(line))
     return 0
 
@@ -421,23 +456,25 @@ def ensemble_specs(nruns, seed=0):
     return out
 
 
-def run_ensemble(args, world, rank, local):
+def ensemble_measure(args, world, rank, local, nruns, steps):
     """Weibel ensemble: many independent runs advanced together (one launch
     per phase over all runs, CUDA-graph replay) vs the same runs each advanced
     through its own graph, one after another and all at once on separate
-    streams.  Metric: aggregate run-steps per second, timed on the device."""
+    streams.  Metric: aggregate run-steps per second, timed on the device.
+    Returns the measurement as a dict (rank 0), None elsewhere."""
     import torch
     import zpic_b200 as zb
     torch.cuda.set_device(local)
-    steps = args.steps if args.steps_given else 500
-    specs = ensemble_specs(args.runs)
+    specs = ensemble_specs(nruns)
     specs = specs[rank::world]                  # runs shard across ranks, no exchange
     sims = []
+    h0 = time.perf_counter()
     for n, p, uz, uth in specs:
         s = zb.Simulation((n // TILE, n // TILE), (TILE, TILE), (n * DX, n * DX), DT, device=local)
         s.add_species(-1.0, (p, p), udist=('thermalcorr', (uth, uth, uth), (0, 0, uz)))
         s.add_species(1.0, (p, p), udist=('thermalcorr', (uth, uth, uth), (0, 0, -uz)))
         sims.append(apply_options(s, args))
+    setup_s = time.perf_counter() - h0
     nparticles = sum(s.np_total(0) + s.np_total(1) for s in sims)
     batch = zb.Batch(sims)
     # device timing: events on one stream that every participating stream
@@ -467,7 +504,8 @@ def run_ensemble(args, world, rank, local):
     batch.advance(args.warmup)
     batch.synchronize()
     l0 = batch.launch_count()
-    tb = timed([bstream], lambda: batch.advance(steps))
+    with ClockSampler(local) as clk:
+        tb = timed([bstream], lambda: batch.advance(steps))
     batch.synchronize()
     launches = batch.launch_count() - l0
     # plain: each run advanced on its own through its own CUDA graph, the runs
@@ -496,25 +534,40 @@ def run_ensemble(args, world, rank, local):
     tc = timed(sstreams, concurrent)
     for s in sims:
         s.synchronize()
-    if rank == 0:
-        print(json.dumps({
-            'metric': 'ensemble_run_steps_per_second', 'value': args.runs * steps / tb,
-            'unit': 'run-steps/s', 'n_gpus': world, 'steps': steps, 'warmup': args.warmup,
-            'ms_per_step': tb / steps * 1e3, 'higher_is_better': True, 'scaling': 'weak',
-            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded)',
-            'config': {'workload': 'Weibel ensemble, %d runs (seeded PCG64 draw of N, ppc, ufl, uth)' % args.runs,
-                       'particles_per_rank': nparticles, 'runs_per_rank': len(sims)},
-            'plain': {'value': args.runs * steps / tp, 'unit': 'run-steps/s',
-                      'how': 'each run through its own CUDA graph, runs one after another'},
-            'plain_concurrent': {'value': args.runs * steps / tc, 'unit': 'run-steps/s',
-                                 'how': 'each run through its own CUDA graph on its own stream, all issued at once'},
-            'batched_over_plain': tp / tb,
-            'batched_over_plain_concurrent': tc / tb,
-            'pushes_per_second': nparticles * world * steps / tb,
-            'gpu_launches': launches,
-            'ctas_per_tile': chunks if chunks is not None else 'automatic',
-        }))
     batch.close()
+    for s in sims:
+        s.close()
+    if rank != 0:
+        return None
+    return {
+        'metric': 'ensemble_run_steps_per_second', 'value': nruns * steps / tb,
+        'unit': 'run-steps/s', 'steps': steps, 'warmup': args.warmup,
+        'ms_per_step': tb / steps * 1e3,
+        'config': {'workload': 'Weibel ensemble, %d runs (seeded PCG64 draw of N, ppc, ufl, uth), '
+                               '%d steps' % (nruns, steps),
+                   'particles_per_rank': nparticles, 'runs_per_rank': len(sims)},
+        'plain': {'value': nruns * steps / tp, 'unit': 'run-steps/s',
+                  'how': 'each run through its own CUDA graph, runs one after another'},
+        'plain_concurrent': {'value': nruns * steps / tc, 'unit': 'run-steps/s',
+                             'how': 'each run through its own CUDA graph on its own stream, all issued at once'},
+        'batched_over_plain': tp / tb,
+        'batched_over_plain_concurrent': tc / tb,
+        'pushes_per_second': nparticles * world * steps / tb,
+        'gpu_launches': launches,
+        'ctas_per_tile': chunks if chunks is not None else 'automatic',
+        'setup_s': setup_s,
+        'clocks': clk.summary(),
+    }
+
+
+def run_ensemble(args, world, rank, local):
+    steps = args.steps if args.steps_given else ENSEMBLE_STEPS
+    ens = ensemble_measure(args, world, rank, local, args.runs, steps)
+    if rank == 0:
+        line = dict(ens)
+        line.update({'n_gpus': world, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+                     'dtype': 'f32', 'data': 'synthetic (reference RNG, seeded)'})
+        print(json.dumps(line))
     return 0
 
 
@@ -654,9 +707,12 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--cells', type=int, default=NCELL, help='grid size (cells per side)')
-    ap.add_argument('--ref-cells', type=int, default=512, help='CPU sample size (cells per side)')
+    ap.add_argument('--ref-cells', type=int, default=512, help='cpu_baseline sample size (cells per side)')
+    ap.add_argument('--reference-cells', type=int, default=NCELL,
+                    help='--impl reference: grid size (cells per side; default the workload itself)')
     ap.add_argument('--ref-steps', type=int, default=10)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-ensemble', action='store_true', help='plasma workload only (skip the ensemble half)')
     ap.add_argument('--autotune', type=int, default=1, help='ensemble: autotune CTAs per tile first (1/0)')
     ap.add_argument('--reorder', type=int, default=None,
                     help='steps between in-tile particle reorders (library option "reorder"; default: the library default)')

@@ -1766,6 +1766,33 @@ void osim_species_tile_sort( osim * s, int sp ) {
     tile_sort( p->part, p->tmp, &p->sort, NULL );
 }
 
+/* Test support, no reference counterpart: puts every clock of the
+ * simulation -- its own iteration count and those of the fields, the current
+ * and each species, and their moving windows' move counts -- where k steps of
+ * osim_advance / osim_advance_mov_window from t = 0 leave them, doing none of
+ * the steps' work.  The rules are the ones the steps apply:
+ * species_advance_mov_window (species.cpp:2083-2128), current_advance
+ * (current.cpp:227-246), emf_advance + emf_move_window (emf.cpp:120-129,
+ * 575-579).  Used to continue from a state taken at step k. */
+void osim_set_clock( osim * s, unsigned k ) {
+    oemf * f = &s->emf; ocur * c = &s->cur;
+    f->iter = 0; f->mw.n_move = 0;
+    c->iter = 0; c->mw.n_move = 0;
+    for ( int i = 0; i < s->nsp; i++ ) { s->sp[i]->iter = 0; s->sp[i]->mw.n_move = 0; }
+    for ( unsigned n = 0; n < k; n++ ) {
+        for ( int i = 0; i < s->nsp; i++ ) {
+            ospecies * sp = s->sp[i];
+            if ( mw_needs_move( &sp->mw, (double) ( ( sp->iter + 1 ) * sp->dt ) ) ) mw_advance( &sp->mw );
+            sp->iter++;
+        }
+        c->iter++;
+        if ( mw_needs_move( &c->mw, c->iter * c->dt ) ) mw_advance( &c->mw );
+        f->iter += 1;
+        if ( f->mw.active && mw_needs_move( &f->mw, f->iter * f->dt ) ) mw_advance( &f->mw );
+    }
+    s->iter = k;
+}
+
 unsigned osim_iter( osim * s ) { return s->iter; }
 uint64_t osim_nmove( osim * s ) {
     uint64_t n = 0;

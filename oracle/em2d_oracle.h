@@ -59,6 +59,7 @@ void     osim_species_move( osim * s, int sp );
 void     osim_species_process_bc( osim * s, int sp );
 void     osim_species_tile_sort( osim * s, int sp );
 
+void     osim_set_clock( osim * s, unsigned k );
 unsigned osim_iter( osim * s );
 uint64_t osim_nmove( osim * s );
 double   osim_species_energy( osim * s, int sp );

@@ -98,6 +98,8 @@ class _Sim:
         RP = ctypes.POINTER(ctypes.c_float if real == 'f32' else ctypes.c_double)
         pre = 'osim_' if self.prefix == 'osim_' else 'ref_'
         self.f = {}
+        if pre == 'osim_':
+            self.f['set_clock'] = self._fn('set_clock', None, [P, U])
         tab = {
             'sim_create' if pre == 'ref_' else 'create': (P, [U, U, U, U, F, F, D]),
             'sim_destroy' if pre == 'ref_' else 'destroy': (None, [P]),
@@ -231,6 +233,12 @@ class _Sim:
 
     def species_tile_sort(self, sp):
         self.f['species_tile_sort'](self.h, sp)
+
+    def set_clock(self, k):
+        """Oracle only: every clock (iterations, window moves) as k steps from
+        t = 0 leave them; with set_particles / set_grid this continues a
+        state taken at step k."""
+        self.f['set_clock'](self.h, int(k))
 
     # ---- diagnostics ----
     def iter(self):

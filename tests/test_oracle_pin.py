@@ -182,3 +182,35 @@ def test_fp64_oracle_tracks_fp32():
     o64.advance(50)
     e32, e64 = energies(o32), energies(o64)
     assert np.all(np.abs(e32[:2] - e64[:2]) <= 1e-4 * np.abs(e64[:2]))
+
+
+def test_oracle_continues_from_a_taken_state():
+    """set_clock (with set_particles / set_grid) restarts the oracle at step k
+    exactly where its own uninterrupted run stands: the next steps agree bit
+    for bit, across window moves (the check the GPU parity tests rely on
+    when they continue the oracle from the library's state)."""
+    geom = ((16, 4), (16, 16), (256 * 0.025, 64 * 0.1), 0.022)
+    run = lwfa_small(OracleSim(*geom))
+    for k in (7, 20, 41):
+        run.advance_mov_window(k - run.iter())
+        cont = lwfa_small(OracleSim(*geom))
+        for sp in range(run.nsp):
+            cont.set_particles(sp, *run.particles(sp))
+        for w in 'EB':
+            cont.set_grid(w, run.grid(w))
+        cont.set_clock(k)
+        assert cont.iter() == k
+        for s in (run, cont):
+            s.advance_mov_window(3)
+        assert_same_state(run, cont)
+    w = weibel(OracleSim((4, 4), (16, 16), (6.4, 6.4), 0.07), (2, 2))
+    w.advance(5)
+    c = weibel(OracleSim((4, 4), (16, 16), (6.4, 6.4), 0.07), (2, 2))
+    for sp in range(2):
+        c.set_particles(sp, *w.particles(sp))
+    for g in 'EB':
+        c.set_grid(g, w.grid(g))
+    c.set_clock(5)
+    w.advance(2)
+    c.advance(2)
+    assert_same_state(w, c)

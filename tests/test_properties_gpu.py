@@ -76,3 +76,27 @@ def test_repack_path_free_streaming():
             assert same_multisets(o.particles(0), g.particles(0)), 'step %d' % n
     # the slab moved into tiles that were empty at the start
     assert set(np.nonzero(o.tiles(0)[0])[0]) - occupied0
+
+
+@pytest.mark.parametrize('ntiles,bc', [
+    ((1, 1), (1, 1, 1, 1)), ((2, 1), (1, 1, 1, 1)), ((1, 2), (1, 1, 1, 1)), ((3, 5), (1, 1, 1, 1)),
+    ((3, 5), (0, 0, 1, 1)), ((4, 3), (0, 0, 0, 0)), ((4, 3), (1, 1, 0, 0)),
+])
+def test_sort_geometries_free_streaming(ntiles, bc):
+    """The tile sort on a hot plasma (many leavers, diagonal ones included)
+    for tilings where a tile is its own neighbour (1 tile along an axis) or
+    two directions lead to the same neighbour (2 tiles), with periodic and
+    open edges: free streaming keeps every particle bit-exact, so the
+    per-tile multisets must match the oracle's at every step."""
+    geom = (ntiles, (8, 8), (ntiles[0] * 0.8, ntiles[1] * 0.8), 0.05)
+
+    def setup(s):
+        s.add_species(-1.0, (3, 2), udist=('thermal', (0.4, 0.3, 0.1), (0.2, -0.1, 0.0)), bc=bc)
+        return s
+    o, g = setup(OracleSim(*geom)), setup(zb.Simulation(*geom))
+    for n in range(1, 31):
+        o.species_advance_free(0)
+        g.species_advance(0, zb.ADVANCE_FREE)
+        assert same_multisets(o.particles(0), g.particles(0)), 'step %d' % n
+    if bc[0] == 0:
+        assert o.tiles(0)[0].sum() < 64 * ntiles[0] * ntiles[1] * 6   # particles left through open edges

@@ -24,7 +24,7 @@
 
 namespace zb {
 struct TileItem { int run; int tile; };
-size_t particle_smem_bytes( int tile_vol, int jacc );
+size_t particle_smem_bytes( int tile_vol, int jacc, int sortw );
 size_t yee_smem_bytes( int tile_vol );
 cudaError_t launch_particles( cudaStream_t, int, int, int, const Item *, int, const SpDev *, const RunDev *, const int *,
                               int, int, int );
@@ -137,10 +137,11 @@ struct HSpecies {
     unsigned * mw_nmove_d = nullptr;   // device copy of the window's move count
 
     void free_all() {
-        PartArrays * arrs[3] = { &d.A, &d.B, &d.S };
+        PartArrays * arrs[2] = { &d.A, &d.B };
         for ( auto * a : arrs ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
         dfree( d.np ); dfree( d.off ); dfree( d.cap ); dfree( d.nidx ); dfree( d.idx );
-        dfree( d.aux ); dfree( d.aux2 ); dfree( d.in_cnt ); dfree( d.stage_off ); dfree( d.stage_cnt );
+        dfree( d.aux ); dfree( d.aux2 ); dfree( d.in_cnt ); dfree( d.stage_cnt );
+        dfree( d.cnt ); dfree( d.base ); dfree( d.hs ); dfree( d.overflow ); dfree( d.sw_ctr );
         dfree( d.new_off ); dfree( d.new_cap ); dfree( d.new_np ); dfree( d.extra ); dfree( d.mode );
         dfree( d.energy ); dfree( d.nmove ); dfree( inj_dyn ); dfree( mw_nmove_d );
     }
@@ -367,7 +368,7 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
         P.max_guard = std::max( P.max_guard, s->run.extx * s->run.exty - s->run.nxx * s->run.nxy );
         P.max_tile_cells = std::max( P.max_tile_cells, s->run.nxx * s->run.nxy );
         // a batch reorders as often as its most frequent run asks
-        if ( s->reorder_every > 0 )
+        if ( s->reorder_every > 0 && !( s->nxx == 16 && s->nxy == 16 ) )
             P.reorder_every = P.reorder_every > 0 ? std::min( P.reorder_every, s->reorder_every ) : s->reorder_every;
         // one accumulation mode per plan: the runs' own when they agree
         P.jacc = ( P.jacc < 0 || P.jacc == s->jacc ) ? s->jacc : 2;
@@ -384,6 +385,9 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
             HSpecies * sp = s->species[k];
             SpDev d = sp->d;
             if ( batch_chunks ) { d.nchunk = batch_chunks; d.chunk_target = 0; }
+            // in-tile order restored by the particle kernel's sorted write-back
+            // (16x16 tiles), by the reorder kernel otherwise
+            d.sw_every = P.tile_n == 16 ? s->reorder_every : 0;
             d.run = (int) r;
             const int gi = (int) P.sps_h.size();
             P.sps_h.push_back( d );
@@ -502,7 +506,7 @@ static int run_particles( Plan & P, cudaStream_t st, int push, int move, const i
 
 static int run_sort( Plan & P, cudaStream_t st, int use_extra ) {
     if ( P.n_sp == 0 ) return ZPIC_OK;
-    PhaseScope ps( prof_sim( P ), st, PH_SORT, 3 );
+    PhaseScope ps( prof_sim( P ), st, PH_SORT, 4 );
     DEV( launch_sort( st, P.sort_items_d, P.n_sort, P.sps_d, P.splist_d, P.n_sp, P.runs_d, use_extra ) );
     return ZPIC_OK;
 }
@@ -852,7 +856,7 @@ static int species_upload( zpic_sim * s, HSpecies * sp, const std::vector<int> &
     cudaStreamDestroy( cs );
     for ( size_t i = 0; i < own_ix.size(); i++ ) { dfree( own_ix[i] ); dfree( own_x[i] ); dfree( own_u[i] ); }
     if ( rc != ZPIC_OK ) { dfree( one ); dfree( poff_d ); return rc; }
-    CK( cudaMemsetAsync( sp->d.in_cnt, 0, nt * sizeof( int ), st ) );
+    CK( cudaMemsetAsync( sp->d.cnt, 0, 9 * (size_t) nt * sizeof( int ), st ) );
     CK( cudaMemsetAsync( sp->d.nidx, 0, nt * sizeof( int ), st ) );
     CK( cudaStreamSynchronize( st ) );
     dfree( one ); dfree( poff_d );
@@ -869,14 +873,17 @@ static int species_alloc( zpic_sim * s, HSpecies * sp, uint64_t max_part ) {
     SpDev & d = sp->d;
     d.ntiles = nt;
     d.max_part = (int) max_part;
-    d.stage_cap = (int) std::max<uint64_t>( 65536, max_part / 4 );
     TRY( alloc_arrays( d.A, max_part ) );
     TRY( alloc_arrays( d.B, max_part ) );
-    TRY( alloc_arrays( d.S, d.stage_cap ) );
     TRY( dalloc( &d.np, nt ) ); TRY( dalloc( &d.off, nt ) ); TRY( dalloc( &d.cap, nt ) );
     TRY( dalloc( &d.nidx, nt ) );
     TRY( dalloc( &d.idx, max_part ) ); TRY( dalloc( &d.aux, max_part ) ); TRY( dalloc( &d.aux2, max_part ) );
-    TRY( dalloc( &d.in_cnt, nt ) ); TRY( dalloc( &d.stage_off, nt ) ); TRY( dalloc( &d.stage_cnt, nt ) );
+    TRY( dalloc( &d.in_cnt, nt ) ); TRY( dalloc( &d.stage_cnt, nt ) );
+    TRY( dalloc( &d.cnt, 9 * (size_t) nt ) ); TRY( dalloc( &d.base, 9 * (size_t) nt ) );
+    TRY( dalloc( &d.hs, nt ) ); TRY( dalloc( &d.overflow, 1 ) ); TRY( dalloc( &d.sw_ctr, 1 ) );
+    CK( cudaMemset( d.sw_ctr, 0, sizeof( int ) ) );
+    CK( cudaMemset( d.cnt, 0, 9 * (size_t) nt * sizeof( int ) ) );
+    CK( cudaMemset( d.overflow, 0, sizeof( int ) ) );
     TRY( dalloc( &d.new_off, nt ) ); TRY( dalloc( &d.new_cap, nt ) ); TRY( dalloc( &d.new_np, nt ) );
     TRY( dalloc( &d.extra, nt ) ); TRY( dalloc( &d.mode, 1 ) );
     TRY( dalloc( &sp->inj_dyn, 4 ) ); TRY( dalloc( &sp->mw_nmove_d, 1 ) );
@@ -909,17 +916,15 @@ static int species_grow( zpic_sim * s, HSpecies * h, uint64_t new_max ) {
     if ( s->plan.built && s->plan.side ) CK( cudaStreamSynchronize( s->plan.side ) );
     SpDev & d = h->d;
     const size_t old = h->max_part;
-    const int stage_cap = (int) std::max<uint64_t>( 65536, new_max / 4 );
-    PartArrays A{}, B{}, S{};
+    PartArrays A{}, B{};
     int * idx = nullptr; int * aux = nullptr; int * aux2 = nullptr;
     int rc = alloc_arrays( A, new_max );
     if ( rc == ZPIC_OK ) rc = alloc_arrays( B, new_max );
-    if ( rc == ZPIC_OK ) rc = alloc_arrays( S, stage_cap );
     if ( rc == ZPIC_OK ) rc = dalloc( &idx, new_max );
     if ( rc == ZPIC_OK ) rc = dalloc( &aux, new_max );
     if ( rc == ZPIC_OK ) rc = dalloc( &aux2, new_max );
     if ( rc != ZPIC_OK ) {
-        PartArrays * na[3] = { &A, &B, &S };
+        PartArrays * na[2] = { &A, &B };
         for ( auto * a : na ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
         dfree( idx ); dfree( aux ); dfree( aux2 );
         return rc;
@@ -936,12 +941,11 @@ static int species_grow( zpic_sim * s, HSpecies * h, uint64_t new_max ) {
     }
     CK( cudaMemcpyAsync( idx, d.idx, old * sizeof( int ), cudaMemcpyDeviceToDevice, s->stream ) );
     CK( cudaStreamSynchronize( s->stream ) );
-    PartArrays * olds[3] = { &d.A, &d.B, &d.S };
+    PartArrays * olds[2] = { &d.A, &d.B };
     for ( auto * a : olds ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
     dfree( d.idx ); dfree( d.aux ); dfree( d.aux2 );
-    d.A = A; d.B = B; d.S = S; d.idx = idx; d.aux = aux; d.aux2 = aux2;
+    d.A = A; d.B = B; d.idx = idx; d.aux = aux; d.aux2 = aux2;
     d.max_part = (int) new_max;
-    d.stage_cap = stage_cap;
     h->max_part = (uint32_t) new_max;
     h->grows++;
     // the descriptor copies of this simulation's plan
@@ -1023,7 +1027,7 @@ static int species_kernel( zpic_sim * s, int sp, int push, int move, const int *
     TRY( ensure_plan( s ) );
     HSpecies * h = s->species[sp];
     if ( h->counters_dirty && move ) {
-        DEV( cudaMemsetAsync( h->d.in_cnt, 0, h->ntiles * sizeof( int ), s->stream ) );
+        DEV( cudaMemsetAsync( h->d.cnt, 0, 9 * (size_t) h->ntiles * sizeof( int ), s->stream ) );
         DEV( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
     }
     Plan & P = s->plan;
@@ -1045,14 +1049,14 @@ static int species_sort( zpic_sim * s, int sp, int use_extra ) {
     Plan & P = s->plan;
     if ( !h->sort_pending ) {
         // leaver lists are stale: detect them now (bnd_check, particles.cpp:212-303)
-        DEV( cudaMemsetAsync( h->d.in_cnt, 0, h->ntiles * sizeof( int ), s->stream ) );
+        DEV( cudaMemsetAsync( h->d.cnt, 0, 9 * (size_t) h->ntiles * sizeof( int ), s->stream ) );
         DEV( cudaMemsetAsync( h->d.nidx, 0, h->ntiles * sizeof( int ), s->stream ) );
         PhaseScope ps( s, s->stream, PH_SORT, 1 );
         DEV( launch_particles( s->stream, 0, 0, 1, P.spk1_d + P.sp_k1_off[sp], P.sp_k1_n[sp], P.sps_d, P.runs_d,
                               nullptr, P.max_tile_vol, 0, 0 ) );
     }
     {
-        PhaseScope ps( s, s->stream, PH_SORT, 3 );
+        PhaseScope ps( s, s->stream, PH_SORT, 4 );
         DEV( launch_sort( s->stream, P.sort_items_d + P.sp_sort_off[sp], P.sp_sort_n[sp], P.sps_d,
                          P.splist_d + sp, 1, P.runs_d, use_extra ) );
     }
@@ -1193,7 +1197,7 @@ int zpic_b200_sim_create( uint32_t ntx, uint32_t nty, uint32_t nxx, uint32_t nxy
     {
         // every tile kernel stages whole tiles in shared memory (227 KB per block)
         const int tv = roundup4( ( nxx + 3 ) * ( nxy + 3 ) );
-        const size_t need = std::max( particle_smem_bytes( tv, 1 ), yee_smem_bytes( tv ) );
+        const size_t need = std::max( particle_smem_bytes( tv, 1, nxx == 16 && nxy == 16 ), yee_smem_bytes( tv ) );
         if ( nxx > 1024 || nxy > 1024 || need > 227 * 1024 )
             return fail( ZPIC_E_INVALID, "tile too large: its field tiles do not fit in shared memory" );
     }
@@ -1405,7 +1409,7 @@ int zpic_b200_sim_advance( zpic_sim * s, int32_t nsteps ) {
     // pending fine-grained work must not be mixed with a full step
     for ( auto * sp : s->species ) {
         if ( sp->counters_dirty ) {
-            CK( cudaMemsetAsync( sp->d.in_cnt, 0, sp->ntiles * sizeof( int ), s->stream ) );
+            CK( cudaMemsetAsync( sp->d.cnt, 0, 9 * (size_t) sp->ntiles * sizeof( int ), s->stream ) );
             CK( cudaMemsetAsync( sp->d.nidx, 0, sp->ntiles * sizeof( int ), s->stream ) );
             sp->counters_dirty = false;
         }
@@ -2034,7 +2038,7 @@ int zpic_b200_batch_advance( zpic_batch * b, int32_t nsteps ) {
         CK( cudaStreamWaitEvent( b->stream, b->ev, 0 ) );
         for ( auto * sp : s->species )
             if ( sp->counters_dirty ) {
-                CK( cudaMemsetAsync( sp->d.in_cnt, 0, sp->ntiles * sizeof( int ), b->stream ) );
+                CK( cudaMemsetAsync( sp->d.cnt, 0, 9 * (size_t) sp->ntiles * sizeof( int ), b->stream ) );
                 CK( cudaMemsetAsync( sp->d.nidx, 0, sp->ntiles * sizeof( int ), b->stream ) );
                 sp->counters_dirty = false;
             }

@@ -273,6 +273,38 @@ __device__ __noinline__ void drain_entry( const CrossQueue & Q, int e, float qnx
 // and split/deposited in full-warp passes, so the split runs on full warps
 // (only a third segment, for the rare double crossings, diverges).
 // ---------------------------------------------------------------------------
+// Block-wide exclusive scan of one value per thread; the block total is
+// written to *total (a shared variable) and visible on return.
+template < int NT >
+__device__ __forceinline__ long long block_exscan( long long v, long long * total ) {
+    static_assert( NT % 32 == 0 && NT <= 1024, "block size" );
+    __shared__ long long wsum[ NT / 32 ];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long incl = v;
+#pragma unroll
+    for ( int o = 1; o < 32; o <<= 1 ) {
+        const long long y = __shfl_up_sync( 0xffffffffu, incl, o );
+        if ( lane >= o ) incl += y;
+    }
+    if ( lane == 31 ) wsum[w] = incl;
+    __syncthreads();
+    if ( w == 0 ) {
+        const long long s = ( lane < NT / 32 ) ? wsum[lane] : 0;
+        long long si = s;
+#pragma unroll
+        for ( int o = 1; o < 32; o <<= 1 ) {
+            const long long y = __shfl_up_sync( 0xffffffffu, si, o );
+            if ( lane >= o ) si += y;
+        }
+        if ( lane < NT / 32 ) wsum[lane] = si - s;
+        if ( lane == NT / 32 - 1 ) *total = si;
+    }
+    __syncthreads();
+    const long long r = wsum[w] + incl - v;
+    __syncthreads();
+    return r;
+}
+
 // Target tile index along one axis for a particle leaving through v (periodic
 // wrap, or -1 past an open edge).
 __device__ __forceinline__ int wrap_tile( int v, int n, int periodic ) {
@@ -313,11 +345,22 @@ __device__ __noinline__ void jfix_flush( int * acc, int n, float * __restrict__ 
 // TN > 0 fixes square TN x TN tiles at compile time, so every shared-memory
 // offset of the interpolation and deposit stencils is an immediate; TN = 0
 // reads the tile shape from the run descriptor.
-template < int PUSH, int MOVE, bool DETECT, typename JT = float, int TN = 0 >
+//
+// SORTW (16x16 tiles, push + move + deposit): on the steps the species' sort
+// counter selects (every S.sw_every steps), each block of 512 particles is
+// written back sorted by its new cell (leavers last), through a
+// shared-memory counting sort.  Particles keep their slot while they drift
+// between the cells of their tile, so the 32 lanes of a warp end up in random
+// cells and the shared-memory field gathers and current atomics meet ~3.3-way
+// bank conflicts; sorted blocks put a warp's lanes on ~16 consecutive cells
+// again (distinct banks, pairs of lanes on one address).
+template < int PUSH, int MOVE, bool DETECT, typename JT = float, int TN = 0, bool SORTW = false >
 __global__ void __launch_bounds__( PK_THREADS, 4 )
 k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
              const RunDev * __restrict__ runs, const int * __restrict__ shifts )
 {
+    static_assert( !SORTW || ( TN == 16 && PUSH && MOVE == 2 && PK_PPT * PK_THREADS == 2 * TN * TN ),
+                   "sorted write-back: 16x16 tiles, full step, 512-particle blocks" );
     extern __shared__ __align__( 16 ) unsigned char smem_raw[];
     const Item it = items[ blockIdx.x ];
     const SpDev & S = sps[ it.sp ];
@@ -336,6 +379,11 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     uint64_t * bar = reinterpret_cast<uint64_t *>( sJ + 3 * tv * JW );
     double * sred = reinterpret_cast<double *>( bar + 1 );
     CrossQueue * xq = reinterpret_cast<CrossQueue *>( sred + PK_THREADS / 32 );
+    // sorted write-back: staging of one block (SoA) and the bucket counts
+    constexpr int SWN = PK_PPT * PK_THREADS;
+    uint32_t * st_c = reinterpret_cast<uint32_t *>( xq + PK_THREADS / 32 );
+    float * st_f = reinterpret_cast<float *>( st_c + SWN );
+    int * hist = reinterpret_cast<int *>( st_f + 5 * SWN );
 
     const int np = S.np[ t ];
     const int off = S.off[ t ];
@@ -350,6 +398,10 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
         if ( PUSH && threadIdx.x == 0 ) S.energy[ eidx ] = 0.0;
         return;
     }
+    // leavers per direction (bnd_check's per-direction counts), added to the
+    // tile's counts once per CTA
+    __shared__ int s_dir[9];
+    if ( DETECT && threadIdx.x < 9 ) s_dir[ threadIdx.x ] = 0;
 
     if ( PUSH ) {
         if ( threadIdx.x == 0 ) {
@@ -416,6 +468,8 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     const unsigned lt_mask = ( 1u << lane ) - 1u;
     CrossQueue & Q = xq[ threadIdx.x >> 5 ];
     int qh = 0, qt = 0;                         // warp-uniform ring head / tail
+    // sorted write-back on this step (CTA-uniform)
+    const bool sw = SORTW && S.sw_every > 0 && *S.sw_ctr == 0;
 
     // Groups of FLUSH_PARTICLES: with the fixed-point tile current the
     // accumulators are flushed between groups (at most 3 additions per
@@ -520,14 +574,62 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                     }
                 }
             }
+            int dst[PK_PPT];
+            if ( SORTW && sw ) {
+                // counting sort of the block by new cell: bucket = cell, TN*TN
+                // for particles outside the tile (leavers, flagged ones)
+                constexpr int NB = TN * TN;
+                int key[PK_PPT], rk[PK_PPT];
+                __syncthreads();                  // the previous block's staging has been read
+                for ( int q = threadIdx.x; q <= NB; q += PK_THREADS ) hist[q] = 0;
+                __syncthreads();
 #pragma unroll
-            for ( int k = 0; k < PK_PPT; k++ ) {
-                const int i = b0 + k * PK_THREADS + threadIdx.x;
-                if ( i < end ) {
-                    if ( MOVE ) { pc[i] = c[k]; pxx[i] = x0[k]; pxy[i] = x1[k]; }
-                    if ( PUSH || rxl || rxu ) pux[i] = u0[k];
-                    if ( PUSH || ryl || ryu ) puy[i] = u1[k];
-                    if ( PUSH ) puz[i] = u2[k];
+                for ( int k = 0; k < PK_PPT; k++ ) {
+                    const int i = b0 + k * PK_THREADS + threadIdx.x;
+                    key[k] = -1; rk[k] = 0;
+                    if ( i < end ) {
+                        const int ix = cell_x( c[k] ), iy = cell_y( c[k] );
+                        key[k] = ( ix >= 0 && ix < TN && iy >= 0 && iy < TN ) ? iy * TN + ix : NB;
+                        rk[k] = atomicAdd( &hist[ key[k] ], 1 );
+                    }
+                }
+                __syncthreads();
+                __shared__ long long s_tot;
+                const long long ex = block_exscan< PK_THREADS >( hist[ threadIdx.x ], &s_tot );
+                hist[ threadIdx.x ] = (int) ex;
+                if ( threadIdx.x == 0 ) hist[ NB ] = (int) s_tot;
+                __syncthreads();
+#pragma unroll
+                for ( int k = 0; k < PK_PPT; k++ ) {
+                    dst[k] = k * PK_THREADS + threadIdx.x;
+                    if ( key[k] >= 0 ) {
+                        const int d = hist[ key[k] ] + rk[k];
+                        dst[k] = d;
+                        st_c[d] = c[k];
+                        st_f[d] = x0[k]; st_f[SWN + d] = x1[k];
+                        st_f[2 * SWN + d] = u0[k]; st_f[3 * SWN + d] = u1[k]; st_f[4 * SWN + d] = u2[k];
+                    }
+                }
+                __syncthreads();
+#pragma unroll
+                for ( int k = 0; k < PK_PPT; k++ ) {
+                    const int j = k * PK_THREADS + threadIdx.x, i = b0 + j;
+                    if ( i < end ) {
+                        pc[i] = st_c[j]; pxx[i] = st_f[j]; pxy[i] = st_f[SWN + j];
+                        pux[i] = st_f[2 * SWN + j]; puy[i] = st_f[3 * SWN + j]; puz[i] = st_f[4 * SWN + j];
+                    }
+                }
+            } else {
+#pragma unroll
+                for ( int k = 0; k < PK_PPT; k++ ) {
+                    dst[k] = k * PK_THREADS + threadIdx.x;
+                    const int i = b0 + dst[k];
+                    if ( i < end ) {
+                        if ( MOVE ) { pc[i] = c[k]; pxx[i] = x0[k]; pxy[i] = x1[k]; }
+                        if ( PUSH || rxl || rxu ) pux[i] = u0[k];
+                        if ( PUSH || ryl || ryu ) puy[i] = u1[k];
+                        if ( PUSH ) puz[i] = u2[k];
+                    }
                 }
             }
 
@@ -552,7 +654,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
 #pragma unroll
                     for ( int k = 0; k < PK_PPT; k++ ) {
                         if ( leave_dir[k] != 4 ) {
-                            const int li = b0 + k * PK_THREADS + threadIdx.x;
+                            const int li = b0 + dst[k];
                             S.idx[ off + pos ] = li;
                             // leaver outbox in buffer B (unused outside a repack),
                             // so that the sort reads the leavers coalesced
@@ -561,11 +663,10 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                             if ( PUSH || MOVE ) { S.B.ux[o] = u0[k]; S.B.uy[o] = u1[k]; S.B.uz[o] = u2[k]; }
                             else { S.B.ux[o] = pux[li]; S.B.uy[o] = puy[li]; S.B.uz[o] = puz[li]; }
                             pos++;
-                            // incoming count of the target tile (bnd_check's
-                            // per-direction counts, summed where they are used)
+                            // counted per direction when the target tile exists
                             const int ttx = wrap_tile( tx + leave_dir[k] % 3 - 1, R.ntx, S.perx );
                             const int tty = wrap_tile( ty + leave_dir[k] / 3 - 1, R.nty, S.pery );
-                            if ( ttx >= 0 && tty >= 0 ) atomicAdd( S.in_cnt + tty * R.ntx + ttx, 1 );
+                            if ( ttx >= 0 && tty >= 0 ) atomicAdd( &s_dir[ leave_dir[k] ], 1 );
                         }
                     }
                 }
@@ -596,6 +697,10 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
         sJout = sE;
         __syncthreads();
     }
+    if ( DETECT && threadIdx.x < 9 && threadIdx.x != 4 ) {
+        const int v = s_dir[ threadIdx.x ];
+        if ( v ) atomicAdd( S.cnt + 9 * t + threadIdx.x, v );
+    }
     if ( threadIdx.x == 0 ) {
         if ( PUSH ) {
             double e = 0.0;
@@ -615,106 +720,109 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
 }
 
 // ---------------------------------------------------------------------------
-// Tile sort (particles.cpp:212-614 semantics; slot layout with slack)
+// Tile sort (particles.cpp:212-614 semantics: afterwards every particle sits
+// in the slot of the tile that holds its cell, at positions [0, np) of that
+// slot; the per-tile multiset is what the reference fixes, its order within
+// the tile depends on thread timing there as here).
+//
+// The particle kernel leaves, per tile t: the leavers' payload in the outbox
+// (buffer B at off[t] + k, k < nidx[t]), their slot indices (idx at
+// off[t] + k) and the number leaving in each direction d (cnt[9 t + d],
+// d = 3 (ycross + 1) + xcross + 1, 4 meaning "stays").  Then:
+//   k_sort_check   per tile: incoming per direction from the 8 neighbour
+//                  counts, their offsets (base), the new count, and whether
+//                  it fits the tile's slot;
+//   k_sort_plan    per species: in place (mode 0) if every tile fits, else
+//                  a new slot layout (mode 1, a repack through buffer B);
+//   k_sort_local   per tile: the slots that are empty below the new count
+//                  (leavers' slots, or room after the old count) are listed;
+//                  stayers above the new count move into the first of them,
+//                  the rest are for the incoming particles;
+//   k_sort_scatter per source tile: each leaver goes from the outbox
+//                  straight to its slot in the target tile, at rank
+//                  base(target, direction) + its rank among this tile's
+//                  leavers in that direction -- no staging copy and no
+//                  returning global atomics.
 // ---------------------------------------------------------------------------
 
+// Tile reached from tile t through direction d (wrap or -1 past an open edge).
+__device__ __forceinline__ int neighbor_tile( int t, int d, int ntx, int nty, int perx, int pery ) {
+    const int wx = wrap_tile( t % ntx + d % 3 - 1, ntx, perx );
+    const int wy = wrap_tile( t / ntx + d / 3 - 1, nty, pery );
+    return ( wx >= 0 && wy >= 0 ) ? wy * ntx + wx : -1;
+}
 
-// Block-wide exclusive scan of one value per thread; the block total is
-// written to *total (a shared variable) and visible on return.
-template < int NT >
-__device__ __forceinline__ long long block_exscan( long long v, long long * total ) {
-    static_assert( NT % 32 == 0 && NT <= 1024, "block size" );
-    __shared__ long long wsum[ NT / 32 ];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    long long incl = v;
+constexpr int CHECK_THREADS = 256;
+
+// One thread per (species, tile) item.  Particles arriving at t through
+// direction d come from the neighbour in the opposite direction 8 - d.
+__global__ void __launch_bounds__( CHECK_THREADS )
+k_sort_check( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps,
+              const RunDev * __restrict__ runs, int use_extra )
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if ( i >= nitems ) return;
+    const Item it = items[i];
+    const SpDev & S = sps[ it.sp ];
+    const RunDev & R = runs[ S.run ];
+    const int t = it.tile;
+    int g[9];
 #pragma unroll
-    for ( int o = 1; o < 32; o <<= 1 ) {
-        const long long y = __shfl_up_sync( 0xffffffffu, incl, o );
-        if ( lane >= o ) incl += y;
+    for ( int d = 0; d < 9; d++ ) {
+        const int src = d == 4 ? -1 : neighbor_tile( t, 8 - d, R.ntx, R.nty, S.perx, S.pery );
+        g[d] = src >= 0 ? S.cnt[ 9 * src + d ] : 0;
     }
-    if ( lane == 31 ) wsum[w] = incl;
-    __syncthreads();
-    if ( w == 0 ) {
-        const long long s = ( lane < NT / 32 ) ? wsum[lane] : 0;
-        long long si = s;
+    int in = 0;
 #pragma unroll
-        for ( int o = 1; o < 32; o <<= 1 ) {
-            const long long y = __shfl_up_sync( 0xffffffffu, si, o );
-            if ( lane >= o ) si += y;
-        }
-        if ( lane < NT / 32 ) wsum[lane] = si - s;
-        if ( lane == NT / 32 - 1 ) *total = si;
-    }
-    __syncthreads();
-    const long long r = wsum[w] + incl - v;
-    __syncthreads();
-    return r;
+    for ( int d = 0; d < 9; d++ ) { S.base[ 9 * t + d ] = in; in += g[d]; }
+    const int stay = S.np[t] - S.nidx[t];
+    const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
+    S.in_cnt[t] = in;
+    S.new_np[t] = stay + in;
+    if ( stay + in + ex > S.cap[t] ) atomicOr( S.overflow, 1 );
 }
 
 constexpr int PLAN_THREADS = 1024;
 
-// Sort plan: one CTA per species.  From the incoming counts (summed by the
-// leaver detection) and the stayers of each tile it decides between the
-// in-place path (everything fits its slot and the staging buffer) and a
-// repack, and lays out offsets for either.
+// One CTA per species.  In place (mode 0) unless a tile overflowed its slot;
+// then the repack layout (mode 1): need[t] = new count + injection reserve,
+// rounded up to 4, and the free capacity spread in proportion to
+// need + min_slack (multiples of 4); mode 2 when the buffer cannot hold the
+// new total (ST_CAPACITY: the host grows buffers before that can happen).
 __global__ void __launch_bounds__( PLAN_THREADS )
 k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_list,
              const RunDev * __restrict__ runs, int use_extra )
 {
     const SpDev & S = sps[ species_list[ blockIdx.x ] ];
     const RunDev & R = runs[ S.run ];
+    const int over = *S.overflow;
+    __syncthreads();
+    // steps until the particle kernel's next sorted write-back
+    if ( threadIdx.x == 0 && S.sw_every > 0 ) {
+        const int c = *S.sw_ctr + 1;
+        *S.sw_ctr = c >= S.sw_every ? 0 : c;
+    }
+    if ( !over ) {
+        if ( threadIdx.x == 0 ) *S.mode = 0;
+        return;
+    }
+    if ( threadIdx.x == 0 ) *S.overflow = 0;
     const int nt = S.ntiles;
     const int per = ( nt + PLAN_THREADS - 1 ) / PLAN_THREADS;
     const int t0 = min( nt, (int) threadIdx.x * per ), t1 = min( nt, t0 + per );
     __shared__ long long s_total;
-    __shared__ int s_fit;
-    if ( threadIdx.x == 0 ) s_fit = 1;
-    __syncthreads();
-
-    long long in_sum = 0;
-    int fit = 1;
-    for ( int t = t0; t < t1; t++ ) {
-        const int in = S.in_cnt[t];
-        const int stay = S.np[t] - S.nidx[t];
-        const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
-        S.new_np[t] = stay + in;
-        S.stage_cnt[t] = 0;
-        if ( stay + in + ex > S.cap[t] ) fit = 0;
-        in_sum += in;
-    }
-    if ( !fit ) s_fit = 0;
-    long long total;
-    long long pre = block_exscan< PLAN_THREADS >( in_sum, &s_total );
-    __syncthreads();
-    total = s_total;
-    for ( int t = t0; t < t1; t++ ) { S.stage_off[t] = (int) pre; pre += S.in_cnt[t]; }
-
-    const int repack = !s_fit || total > S.stage_cap;
-    if ( !repack ) {
-        if ( threadIdx.x == 0 ) {
-            *S.mode = 0;
-        }
-        return;
-    }
-    if ( threadIdx.x == 0 && total > S.stage_cap ) atomicOr( R.status, ST_STAGE_OVERFLOW );
-
-    // Repack layout: need[t] rounded up to 4, then the free capacity spread in
-    // proportion to need[t] + min_slack (multiples of 4).
     long long need_sum = 0, w_sum = 0;
     for ( int t = t0; t < t1; t++ ) {
         const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
         const int need = ( S.new_np[t] + ex + 3 ) & ~3;
         need_sum += need;
         w_sum += need + S.min_slack;
+        S.stage_cnt[t] = 0;
     }
-    __syncthreads();
-    long long pre_need = block_exscan< PLAN_THREADS >( need_sum, &s_total );
-    __syncthreads();
+    block_exscan< PLAN_THREADS >( need_sum, &s_total );
     const long long need_total = s_total;
     __syncthreads();
-    (void) pre_need;
     block_exscan< PLAN_THREADS >( w_sum, &s_total );
-    __syncthreads();
     const long long w_total = s_total;
     const long long free_cap = (long long) S.max_part - need_total;
     if ( free_cap < 0 ) {
@@ -745,84 +853,126 @@ constexpr int SORT_THREADS = 256;
 constexpr int SORT_WARPS = SORT_THREADS / 32;
 constexpr int SU = 4;                             // sort entries per lane in flight
 
-// Leavers to staging, then the holes they leave in [0, n0) filled with the
-// stayers found in the tail [n0, np).  WPT warps per tile (1 when there are
-// many tiles, a whole CTA when there are few and they are large): the hole
-// and stayer lists are compacted with ballots and appended through per-tile
-// shared counters, then paired by rank (any pairing of holes and tail
-// stayers is valid; with one warp per tile it is in particle order).
+// Repack, first half (mode 1): every particle of the species goes to buffer B
+// in the new slot layout -- stayers into their own tile's new slot, leavers
+// into their target's.  The whole grid strides over the particle buffer (a
+// tile's particles are spread over all CTAs, however unevenly the tiles are
+// filled); slots are claimed per destination with one atomic per group of
+// lanes sharing it.
+__device__ void repack_out( const SpDev & S, const RunDev & R ) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = ( 1u << lane ) - 1u;
+    const int nt = S.ntiles, ntx = R.ntx, nty = R.nty, nxx = R.nxx, nxy = R.nxy;
+    const long long n = S.max_part;
+    for ( long long p0 = (long long) blockIdx.x * blockDim.x; p0 < n; p0 += (long long) gridDim.x * blockDim.x ) {
+        const long long p = p0 + threadIdx.x;
+        int dest = -1, ix = 0, iy = 0, xc = 0, yc = 0;
+        if ( p < n ) {
+            // tile of slot p: the last tile whose slot starts at or before p
+            int lo = 0, hi = nt - 1;
+            while ( lo < hi ) {
+                const int mid = ( lo + hi + 1 ) >> 1;
+                if ( S.off[mid] <= p ) lo = mid; else hi = mid - 1;
+            }
+            const int t = lo, i = (int) ( p - S.off[t] );
+            if ( i >= 0 && i < S.np[t] ) {
+                const uint32_t c = S.A.cell[p];
+                ix = cell_x( c ); iy = cell_y( c );
+                xc = ( ix >= nxx ) - ( ix < 0 ); yc = ( iy >= nxy ) - ( iy < 0 );
+                const int ttx = wrap_tile( t % ntx + xc, ntx, S.perx ), tty = wrap_tile( t / ntx + yc, nty, S.pery );
+                dest = ( ttx >= 0 && tty >= 0 ) ? tty * ntx + ttx : -1;
+            }
+        }
+        const unsigned same = __match_any_sync( 0xffffffffu, dest );
+        const int leader = __ffs( same ) - 1;
+        int base = 0;
+        if ( dest >= 0 && lane == leader ) base = atomicAdd( S.stage_cnt + dest, __popc( same ) );
+        base = __shfl_sync( same, base, leader );
+        if ( dest >= 0 ) {
+            const size_t d = (size_t) S.new_off[dest] + base + __popc( same & lt );
+            copy_particle( S.B, d, S.A, (size_t) p );
+            if ( xc != 0 || yc != 0 ) S.B.cell[d] = pack_cell( ix - xc * nxx, iy - yc * nxy );
+        }
+    }
+}
+
+// Repack, second half: B -> A over the whole buffer (slack included),
+// 16-byte vectors (the arrays are cudaMalloc'd, 256-byte aligned); the last
+// max_part % 4 entries are copied singly.
+__device__ __forceinline__ void copy_vec( void * dst, const void * src, long long i ) {
+    reinterpret_cast<uint4 *>( dst )[i] = reinterpret_cast<const uint4 *>( src )[i];
+}
+
+__device__ void repack_in( const SpDev & S ) {
+    const long long n = S.max_part, n4 = n / 4;
+    const long long stride = (long long) gridDim.x * blockDim.x;
+    for ( long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride ) {
+        copy_vec( S.A.cell, S.B.cell, i ); copy_vec( S.A.xx, S.B.xx, i ); copy_vec( S.A.xy, S.B.xy, i );
+        copy_vec( S.A.ux, S.B.ux, i );     copy_vec( S.A.uy, S.B.uy, i ); copy_vec( S.A.uz, S.B.uz, i );
+    }
+    for ( long long p = 4 * n4 + blockIdx.x * (long long) blockDim.x + threadIdx.x; p < n; p += stride )
+        copy_particle( S.A, (size_t) p, S.B, (size_t) p );
+}
+
+// Per tile (WPT warps per tile; 1 when there are many tiles, a whole CTA when
+// there are few and they are large): with nn = np - nidx + in the new count,
+// list the slots that will be empty below nn -- the leavers' slots below nn
+// (aux, appended through a per-tile shared counter from warp ballots), then
+// np .. nn-1 when the tile grows -- and the stayers at or above nn (aux2).
+// Stayer q moves into empty slot q; the remaining entries, from hs = number of
+// such stayers on, receive the incoming particles (k_sort_scatter).  Also
+// clears the tile's direction counts for the next step (k_sort_check has read
+// them).  Species in mode 1 are repacked instead (first half).
 template < int WPT >
 __global__ void __launch_bounds__( SORT_THREADS )
-k_sort_out( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps,
-            const RunDev * __restrict__ runs )
+k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps,
+              const int * __restrict__ species_list, int nspecies, const RunDev * __restrict__ runs )
 {
     constexpr int TPB = SORT_WARPS / WPT;         // tiles per CTA
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tib = warp / WPT, sub = warp % WPT;
     const unsigned lt = ( 1u << lane ) - 1u;
-    __shared__ int s_nh[TPB], s_ns[TPB];
-    // one tile per warp (WPT 1): the warp's own counters, warp-level syncs
-    if ( sub == 0 && lane == 0 ) { s_nh[tib] = 0; s_ns[tib] = 0; }
+    __shared__ int s_ne[TPB], s_ns[TPB];
+    if ( sub == 0 && lane == 0 ) { s_ne[tib] = 0; s_ns[tib] = 0; }
     if ( WPT > 1 ) __syncthreads(); else __syncwarp();
 
     const int wi = blockIdx.x * TPB + tib;
     bool active = wi < nitems;
     Item it{};
     const SpDev * Sp = nullptr;
-    const RunDev * Rp = nullptr;
     if ( active ) {
         it = items[ wi ];
         Sp = &sps[ it.sp ];
-        Rp = &runs[ Sp->run ];
-        active = *Sp->mode == 0;              // repacks: k_repack_out
+        if ( sub == 0 && lane < 9 ) Sp->cnt[ 9 * it.tile + lane ] = 0;
+        active = *Sp->mode == 0;
     }
-    int t = 0, ntx = 1, nty = 1, nxx = 1, nxy = 1, tx = 0, ty = 0, np = 0, nl = 0, n0 = 0, off = 0;
-    if ( active ) {
-        t = it.tile; ntx = Rp->ntx; nty = Rp->nty; nxx = Rp->nxx; nxy = Rp->nxy;
-        tx = t % ntx; ty = t / ntx;
-        np = Sp->np[t]; nl = Sp->nidx[t]; n0 = np - nl; off = Sp->off[t];
-    }
+    int t = 0, np = 0, nl = 0, nn = 0, off = 0, nxx = 1, nxy = 1;
     if ( active ) {
         const SpDev & S = *Sp;
-        // SU entries per lane in flight: the dependent loads (index, cell,
-        // particle) of SU leavers are issued together; leaver k's data sits
-        // in the outbox (buffer B) at off + k
+        const RunDev & R = runs[ S.run ];
+        t = it.tile; nxx = R.nxx; nxy = R.nxy;
+        np = S.np[t]; nl = S.nidx[t]; off = S.off[t];
+        nn = np - nl + S.in_cnt[t];
+        // leavers' slots below nn, SU per lane in flight
         for ( int k0 = sub * 32 * SU; k0 < nl; k0 += WPT * 32 * SU ) {
-            int i[SU]; uint32_t c[SU];
+            int i[SU];
 #pragma unroll
             for ( int u = 0; u < SU; u++ ) {
                 const int k = k0 + u * 32 + lane;
-                i[u] = k < nl ? S.idx[ off + k ] : -1;
-                c[u] = k < nl ? S.B.cell[ (size_t) off + k ] : 0u;
+                i[u] = k < nl ? S.idx[ off + k ] : nn;
             }
 #pragma unroll
             for ( int u = 0; u < SU; u++ ) {
-                if ( i[u] >= 0 ) {
-                    const size_t g = (size_t) off + k0 + u * 32 + lane;
-                    const int ix = cell_x( c[u] ), iy = cell_y( c[u] );
-                    const int xc = ( ix >= nxx ) - ( ix < 0 ), yc = ( iy >= nxy ) - ( iy < 0 );
-                    const int ttx = wrap_tile( tx + xc, ntx, S.perx ), tty = wrap_tile( ty + yc, nty, S.pery );
-                    if ( ttx >= 0 && tty >= 0 ) {
-                        const int tt = tty * ntx + ttx;
-                        const int slot = atomicAdd( S.stage_cnt + tt, 1 );
-                        const size_t d = (size_t) S.stage_off[tt] + slot;
-                        S.S.cell[d] = pack_cell( ix - xc * nxx, iy - yc * nxy );
-                        S.S.xx[d] = S.B.xx[g]; S.S.xy[d] = S.B.xy[g];
-                        S.S.ux[d] = S.B.ux[g]; S.S.uy[d] = S.B.uy[g]; S.S.uz[d] = S.B.uz[g];
-                    }
-                }
-            }
-#pragma unroll
-            for ( int u = 0; u < SU; u++ ) {
-                const bool hole = i[u] >= 0 && i[u] < n0;
-                const unsigned m = __ballot_sync( 0xffffffffu, hole );
-                int base = 0;
-                if ( lane == 0 && m ) base = atomicAdd( &s_nh[tib], __popc( m ) );
-                base = __shfl_sync( 0xffffffffu, base, 0 );
-                if ( hole ) S.aux[ off + base + __popc( m & lt ) ] = i[u];
+                const bool e = i[u] < nn;
+                const unsigned m = __ballot_sync( 0xffffffffu, e );
+                int b = 0;
+                if ( lane == 0 && m ) b = atomicAdd( &s_ne[tib], __popc( m ) );
+                b = __shfl_sync( 0xffffffffu, b, 0 );
+                if ( e ) S.aux[ off + b + __popc( m & lt ) ] = i[u];
             }
         }
-        for ( int c0 = n0 + sub * 32 * SU; c0 < np; c0 += WPT * 32 * SU ) {
+        // stayers at or above nn
+        for ( int c0 = nn + sub * 32 * SU; c0 < np; c0 += WPT * 32 * SU ) {
             uint32_t c[SU];
 #pragma unroll
             for ( int u = 0; u < SU; u++ ) {
@@ -834,141 +984,149 @@ k_sort_out( const Item * __restrict__ items, int nitems, const SpDev * __restric
                 const int ix = cell_x( c[u] ), iy = cell_y( c[u] );
                 const bool stay = ix >= 0 && ix < nxx && iy >= 0 && iy < nxy;
                 const unsigned m = __ballot_sync( 0xffffffffu, stay );
-                int base = 0;
-                if ( lane == 0 && m ) base = atomicAdd( &s_ns[tib], __popc( m ) );
-                base = __shfl_sync( 0xffffffffu, base, 0 );
-                if ( stay ) S.aux2[ off + base + __popc( m & lt ) ] = c0 + u * 32 + lane;
+                int b = 0;
+                if ( lane == 0 && m ) b = atomicAdd( &s_ns[tib], __popc( m ) );
+                b = __shfl_sync( 0xffffffffu, b, 0 );
+                if ( stay ) S.aux2[ off + b + __popc( m & lt ) ] = c0 + u * 32 + lane;
             }
         }
     }
     if ( WPT > 1 ) __syncthreads(); else __syncwarp();
     if ( active ) {
         const SpDev & S = *Sp;
-        const int nh = s_nh[tib], ns = s_ns[tib], nh2 = min( nh, ns );
-        if ( sub == 0 && lane == 0 && nh != ns ) atomicOr( Rp->status, ST_BAD_CELL );
-        for ( int r0 = sub * 32 * SU; r0 < nh2; r0 += WPT * 32 * SU ) {
+        const int ne = s_ne[tib], ns = s_ns[tib];
+        // every empty slot below nn receives one particle: a stayer from above
+        // nn or an incoming one (inconsistent counts are reported and the
+        // tile's lists are not used)
+        if ( ne + max( 0, nn - np ) != ns + S.in_cnt[t] ) {
+            if ( sub == 0 && lane == 0 ) { S.hs[t] = nn; atomicOr( runs[ S.run ].status, ST_BAD_CELL ); }
+            active = false;
+        }
+    }
+    if ( active ) {
+        const SpDev & S = *Sp;
+        const int ne = s_ne[tib], ns = s_ns[tib];
+        // the room after the old count, when the tile grows
+        for ( int j = sub * 32 + lane; j < nn - np; j += WPT * 32 ) S.aux[ off + ne + j ] = np + j;
+        // stayers above nn into the first empty slots (pairs by list rank)
+        for ( int r0 = sub * 32 * SU; r0 < ns; r0 += WPT * 32 * SU ) {
             int h[SU], src[SU];
 #pragma unroll
             for ( int u = 0; u < SU; u++ ) {
                 const int r = r0 + u * 32 + lane;
-                h[u] = r < nh2 ? S.aux[ off + r ] : -1;
-                src[u] = r < nh2 ? S.aux2[ off + r ] : -1;
+                h[u] = r < ns ? S.aux[ off + r ] : -1;
+                src[u] = r < ns ? S.aux2[ off + r ] : -1;
             }
 #pragma unroll
             for ( int u = 0; u < SU; u++ )
                 if ( h[u] >= 0 ) copy_particle( S.A, (size_t) off + h[u], S.A, (size_t) off + src[u] );
         }
-        if ( sub == 0 && lane == 0 ) S.np[t] = n0;
+        if ( sub == 0 && lane == 0 ) S.hs[t] = ns;
     }
-}
-
-// Repack (sort plan mode 1): every particle of the species goes to buffer B
-// in the new slot layout -- stayers into their own tile's new slot, leavers
-// into their target's -- then B is copied back to A.  These kernels run on a
-// fixed grid of CTAs striding over the whole particle buffer (a tile's
-// particles are spread over all CTAs, however unevenly the tiles are filled)
-// and return at once when no species of the list repacks.  Slots are claimed
-// per destination with one atomic per group of lanes sharing it.
-constexpr int REPACK_THREADS = 256;
-
-__global__ void __launch_bounds__( REPACK_THREADS )
-k_repack_out( const SpDev * __restrict__ sps, const int * __restrict__ species_list, int nspecies,
-              const RunDev * __restrict__ runs )
-{
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = ( 1u << lane ) - 1u;
     for ( int k = 0; k < nspecies; k++ ) {
         const SpDev & S = sps[ species_list[k] ];
-        if ( *S.mode != 1 ) continue;
-        const RunDev & R = runs[ S.run ];
-        const int nt = S.ntiles, ntx = R.ntx, nty = R.nty, nxx = R.nxx, nxy = R.nxy;
-        const long long n = S.max_part;
-        for ( long long p0 = (long long) blockIdx.x * blockDim.x; p0 < n; p0 += (long long) gridDim.x * blockDim.x ) {
-            const long long p = p0 + threadIdx.x;
-            int dest = -1, ix = 0, iy = 0, xc = 0, yc = 0;
-            if ( p < n ) {
-                // tile of slot p: the last tile whose slot starts at or before p
-                int lo = 0, hi = nt - 1;
-                while ( lo < hi ) {
-                    const int mid = ( lo + hi + 1 ) >> 1;
-                    if ( S.off[mid] <= p ) lo = mid; else hi = mid - 1;
-                }
-                const int t = lo, i = (int) ( p - S.off[t] );
-                if ( i >= 0 && i < S.np[t] ) {
-                    const uint32_t c = S.A.cell[p];
-                    ix = cell_x( c ); iy = cell_y( c );
-                    xc = ( ix >= nxx ) - ( ix < 0 ); yc = ( iy >= nxy ) - ( iy < 0 );
-                    const int ttx = wrap_tile( t % ntx + xc, ntx, S.perx ), tty = wrap_tile( t / ntx + yc, nty, S.pery );
-                    dest = ( ttx >= 0 && tty >= 0 ) ? tty * ntx + ttx : -1;
-                }
-            }
-            const unsigned same = __match_any_sync( 0xffffffffu, dest );
-            const int leader = __ffs( same ) - 1;
-            int base = 0;
-            if ( dest >= 0 && lane == leader ) base = atomicAdd( S.stage_cnt + dest, __popc( same ) );
-            base = __shfl_sync( same, base, leader );
-            if ( dest >= 0 ) {
-                const size_t d = (size_t) S.new_off[dest] + base + __popc( same & lt );
-                copy_particle( S.B, d, S.A, (size_t) p );
-                if ( xc != 0 || yc != 0 ) S.B.cell[d] = pack_cell( ix - xc * nxx, iy - yc * nxy );
-            }
-        }
+        if ( *S.mode == 1 ) repack_out( S, runs[ S.run ] );
     }
 }
 
-// B -> A over the whole buffer (slack included), 16-byte vectors: the six
-// arrays are cudaMalloc'd (256-byte aligned); the last max_part % 4 entries
-// are copied singly.
-__device__ __forceinline__ void copy_vec( void * dst, const void * src, long long n4, long long i ) {
-    if ( i < n4 ) reinterpret_cast<uint4 *>( dst )[i] = reinterpret_cast<const uint4 *>( src )[i];
-}
-
-__global__ void __launch_bounds__( REPACK_THREADS )
-k_repack_in( const SpDev * __restrict__ sps, const int * __restrict__ species_list, int nspecies )
-{
-    for ( int k = 0; k < nspecies; k++ ) {
-        const SpDev & S = sps[ species_list[k] ];
-        if ( *S.mode != 1 ) continue;
-        const long long n = S.max_part, n4 = n / 4;
-        const long long stride = (long long) gridDim.x * blockDim.x;
-        for ( long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride ) {
-            copy_vec( S.A.cell, S.B.cell, n4, i ); copy_vec( S.A.xx, S.B.xx, n4, i ); copy_vec( S.A.xy, S.B.xy, n4, i );
-            copy_vec( S.A.ux, S.B.ux, n4, i );     copy_vec( S.A.uy, S.B.uy, n4, i ); copy_vec( S.A.uz, S.B.uz, n4, i );
-        }
-        for ( long long p = 4 * n4 + blockIdx.x * (long long) blockDim.x + threadIdx.x; p < n; p += stride )
-            copy_particle( S.A, (size_t) p, S.B, (size_t) p );
-    }
-}
-
-// Incoming particles from staging appended after the stayers (after a repack
-// only the tile's slot is updated: its particles are in place); resets the
-// per-tile counters.  WPT warps per tile, as k_sort_out.
+// Per source tile (WPT warps per tile): each leaver of the outbox goes to
+// slot aux[off[tt] + hs[tt] + base[tt][d] + rank] of its target tt, rank
+// counted per direction d in outbox order (shared counters, one atomic per
+// group of lanes with the same direction).  Then the tile's count becomes the
+// new one.  Species in mode 1 get their new slot layout and the second half
+// of the repack.
 template < int WPT >
 __global__ void __launch_bounds__( SORT_THREADS )
-k_sort_in( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps )
+k_sort_scatter( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps,
+                const int * __restrict__ species_list, int nspecies, const RunDev * __restrict__ runs )
 {
     constexpr int TPB = SORT_WARPS / WPT;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tib = warp / WPT, sub = warp % WPT;
+    const unsigned lt = ( 1u << lane ) - 1u;
+    __shared__ int s_rank[TPB][9];
+    __shared__ int s_off[TPB][9];                 // off[tt] of the target through direction d
+    __shared__ int s_aux[TPB][9];                 // its list position of the first slot for d (-1: dropped)
+    __shared__ int s_cap[TPB][9];                 // new count of the target (bound of its list and slots)
+
     const int wi = blockIdx.x * TPB + tib;
-    if ( wi >= nitems ) return;
-    const Item it = items[ wi ];
-    const SpDev & S = sps[ it.sp ];
-    const int mode = *S.mode;
-    const int t = it.tile;
-    const int n0 = S.np[t];
-    if ( mode == 0 ) {
-        const int in = S.in_cnt[t], off = S.off[t], so = S.stage_off[t];
-#pragma unroll 4
-        for ( int k = sub * 32 + lane; k < in; k += WPT * 32 )
-            copy_particle( S.A, (size_t) off + n0 + k, S.S, (size_t) so + k );
+    bool active = wi < nitems;
+    Item it{};
+    const SpDev * Sp = nullptr;
+    int mode = -1;
+    if ( active ) {
+        it = items[ wi ];
+        Sp = &sps[ it.sp ];
+        mode = *Sp->mode;
+        active = mode == 0;
     }
-    // every warp of the tile has read np before any of them writes it
+    if ( active && sub == 0 && lane < 9 ) {
+        const SpDev & S = *Sp;
+        const RunDev & R = runs[ S.run ];
+        const int tt = lane == 4 ? -1 : neighbor_tile( it.tile, lane, R.ntx, R.nty, S.perx, S.pery );
+        int o = 0, a = -1, nn = 0;
+        if ( tt >= 0 ) {
+            o = S.off[tt];
+            a = S.hs[tt] + S.base[ 9 * tt + lane ];
+            nn = S.new_np[tt];
+        }
+        s_off[tib][lane] = o;
+        s_aux[tib][lane] = a;
+        s_cap[tib][lane] = nn;
+        s_rank[tib][lane] = 0;
+    }
     if ( WPT > 1 ) __syncthreads(); else __syncwarp();
-    if ( sub == 0 && lane == 0 ) {
-        if ( mode == 0 ) S.np[t] = n0 + S.in_cnt[t];
-        else if ( mode == 1 ) { S.np[t] = S.new_np[t]; S.off[t] = S.new_off[t]; S.cap[t] = S.new_cap[t]; }
-        S.in_cnt[t] = 0; S.nidx[t] = 0;
+    if ( active ) {
+        const SpDev & S = *Sp;
+        const RunDev & R = runs[ S.run ];
+        const int t = it.tile, nxx = R.nxx, nxy = R.nxy;
+        const int nl = S.nidx[t], off = S.off[t];
+        for ( int k0 = sub * 32; k0 < nl; k0 += WPT * 32 ) {
+            const int k = k0 + lane;
+            const bool in = k < nl;
+            const size_t g = (size_t) off + k;
+            uint32_t c = 0; float xx = 0.f, xy = 0.f, ux = 0.f, uy = 0.f, uz = 0.f;
+            if ( in ) { c = S.B.cell[g]; xx = S.B.xx[g]; xy = S.B.xy[g]; ux = S.B.ux[g]; uy = S.B.uy[g]; uz = S.B.uz[g]; }
+            const int ix = cell_x( c ), iy = cell_y( c );
+            const int xc = ( ix >= nxx ) - ( ix < 0 ), yc = ( iy >= nxy ) - ( iy < 0 );
+            const int d = in ? ( yc + 1 ) * 3 + xc + 1 : 9;
+            const unsigned peers = __match_any_sync( 0xffffffffu, d );
+            const int leader = __ffs( peers ) - 1;
+            int b = 0;
+            if ( d < 9 && lane == leader ) b = atomicAdd( &s_rank[tib][d], __popc( peers ) );
+            b = __shfl_sync( peers, b, leader );
+            if ( d < 9 && d != 4 ) {
+                const int a = s_aux[tib][d];
+                if ( a >= 0 ) {
+                    // list entry and slot both below the target's new count
+                    // (anything else means inconsistent counts: reported, the
+                    // particle is not written)
+                    const int r = a + b + __popc( peers & lt ), nnt = s_cap[tib][d];
+                    const int slot = r < nnt ? S.aux[ (size_t) s_off[tib][d] + r ] : -1;
+                    if ( slot >= 0 && slot < nnt ) {
+                        const size_t p = (size_t) s_off[tib][d] + slot;
+                        S.A.cell[p] = pack_cell( ix - xc * nxx, iy - yc * nxy );
+                        S.A.xx[p] = xx; S.A.xy[p] = xy;
+                        S.A.ux[p] = ux; S.A.uy[p] = uy; S.A.uz[p] = uz;
+                    } else {
+                        atomicOr( R.status, ST_BAD_CELL );
+                    }
+                }
+            }
+        }
+    }
+    // every warp of the tile has read nidx before it is cleared
+    if ( WPT > 1 ) __syncthreads(); else __syncwarp();
+    if ( ( mode == 0 || mode == 1 ) && sub == 0 && lane == 0 ) {
+        const SpDev & S = *Sp;
+        const int t = it.tile;
+        if ( mode == 0 ) S.np[t] = S.new_np[t];
+        else { S.np[t] = S.new_np[t]; S.off[t] = S.new_off[t]; S.cap[t] = S.new_cap[t]; }
+        S.nidx[t] = 0;
+    }
+    for ( int k = 0; k < nspecies; k++ ) {
+        const SpDev & S = sps[ species_list[k] ];
+        if ( *S.mode == 1 ) repack_in( S );
     }
 }
 
@@ -1407,19 +1565,22 @@ k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, cons
 // ---------------------------------------------------------------------------
 namespace zb {
 
-size_t particle_smem_bytes( int tile_vol, int jacc ) {
+// Shared memory of the particle kernel; sortw adds the staging of the sorted
+// write-back (one 512-particle block, SoA) and its 257 bucket counts.
+size_t particle_smem_bytes( int tile_vol, int jacc, int sortw ) {
     return (size_t) ( jacc ? 12 : 9 ) * tile_vol * sizeof( float ) + 8 + ( PK_THREADS / 32 ) * sizeof( double ) +
-           ( PK_THREADS / 32 ) * sizeof( CrossQueue );
+           ( PK_THREADS / 32 ) * sizeof( CrossQueue ) +
+           ( sortw ? (size_t) PK_PPT * PK_THREADS * 6 * 4 + 260 * 4 : 0 );
 }
 
 typedef void ( *pk_fn )( const Item *, const SpDev *, const RunDev *, const int * );
 
 static pk_fn pick_particle_kernel( int push, int move, int detect, int jacc, int tile_n ) {
     if ( tile_n == 16 && move == 2 && detect && ( push == 1 || push == 2 ) ) {
-        if ( jacc == 0 ) return push == 1 ? k_particles< 1, 2, true, float, 16 > : k_particles< 2, 2, true, float, 16 >;
-        if ( jacc == 1 ) return push == 1 ? k_particles< 1, 2, true, double, 16 > : k_particles< 2, 2, true, double, 16 >;
-        return push == 1 ? k_particles< 1, 2, true, int, 16 >
-                         : k_particles< 2, 2, true, int, 16 >;
+        if ( jacc == 0 ) return push == 1 ? k_particles< 1, 2, true, float, 16, true > : k_particles< 2, 2, true, float, 16, true >;
+        if ( jacc == 1 ) return push == 1 ? k_particles< 1, 2, true, double, 16, true > : k_particles< 2, 2, true, double, 16, true >;
+        return push == 1 ? k_particles< 1, 2, true, int, 16, true >
+                         : k_particles< 2, 2, true, int, 16, true >;
     }
     if ( jacc == 1 && move == 2 ) {
 #define PKD( P, M, D ) if ( push == P && move == M && detect == D ) return k_particles< P, M, D, double >;
@@ -1448,7 +1609,8 @@ cudaError_t launch_particles( cudaStream_t st, int push, int move, int detect, c
     if ( move != 2 ) jacc = 0;
     pk_fn f = pick_particle_kernel( push, move, detect, jacc, tile_n );
     if ( !f ) return cudaErrorInvalidValue;
-    const size_t smem = particle_smem_bytes( max_tile_vol, jacc );
+    const bool sortw = tile_n == 16 && move == 2 && detect && ( push == 1 || push == 2 );
+    const size_t smem = particle_smem_bytes( max_tile_vol, jacc, sortw );
     if ( smem > 48 * 1024 )
         cudaFuncSetAttribute( (const void *) f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
     if ( nitems <= 0 ) return cudaSuccess;
@@ -1459,23 +1621,25 @@ cudaError_t launch_particles( cudaStream_t st, int push, int move, int detect, c
 cudaError_t launch_sort( cudaStream_t st, const Item * items, int nitems, const SpDev * sps,
                          const int * species_list, int nspecies, const RunDev * runs, int use_extra ) {
     if ( nitems <= 0 ) return cudaSuccess;
-    k_sort_plan<<< nspecies, PLAN_THREADS, 0, st >>>( sps, species_list, runs, use_extra );
     int dev = 0, sms = 148;
     cudaGetDevice( &dev );
     cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
+    k_sort_check<<< ( nitems + CHECK_THREADS - 1 ) / CHECK_THREADS, CHECK_THREADS, 0, st >>>( items, nitems, sps, runs,
+                                                                                         use_extra );
+    k_sort_plan<<< nspecies, PLAN_THREADS, 0, st >>>( sps, species_list, runs, use_extra );
     // a warp per tile, unless the tiles are too few to occupy the GPU's SMs
-    // (then they are large, and get a CTA each): 512 tiles of 32x32 in a
-    // filamented Weibel plasma 0.51 -> 0.28 ms per step; 8,192 tiles of a
-    // laser-wakefield run stay faster with a warp each
+    // (then they are large, and get a CTA each); the grid covers the GPU at
+    // least once for the repack's grid-stride loops
     const bool wide = nitems < sms * 16;
     const int tpb = wide ? 1 : SORT_WARPS;
-    const int nb = ( nitems + tpb - 1 ) / tpb;
-    if ( wide ) k_sort_out< SORT_WARPS ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, runs );
-    else        k_sort_out< 1 ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, runs );
-    k_repack_out<<< 8 * sms, REPACK_THREADS, 0, st >>>( sps, species_list, nspecies, runs );
-    k_repack_in<<< 8 * sms, REPACK_THREADS, 0, st >>>( sps, species_list, nspecies );
-    if ( wide ) k_sort_in< SORT_WARPS ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps );
-    else        k_sort_in< 1 ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps );
+    const int nb = std::max( ( nitems + tpb - 1 ) / tpb, 4 * sms );
+    if ( wide ) {
+        k_sort_local< SORT_WARPS ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, species_list, nspecies, runs );
+        k_sort_scatter< SORT_WARPS ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, species_list, nspecies, runs );
+    } else {
+        k_sort_local< 1 ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, species_list, nspecies, runs );
+        k_sort_scatter< 1 ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, species_list, nspecies, runs );
+    }
     return cudaGetLastError();
 }
 

@@ -57,18 +57,20 @@ struct SpDev {
     int chunk_target;             // particles per CTA: a tile uses ceil(np / target) of its
                                   // nchunk CTAs (0: all of them)
     int max_part;                 // capacity of A and B
-    int stage_cap;                // capacity of the staging buffer
-    PartArrays A, B, S;
+    PartArrays A, B;              // particles (tile slots) and second buffer (leaver outbox, repack target)
     int * np; int * off; int * cap;          // tile slots of A
     int * nidx;                   // [ntiles] leavers per tile
     int * idx;                    // [max_part] local index of leavers, at off[t]+k
-    int * aux; int * aux2;        // [max_part] hole / tail lists, at off[t]+k
-    int * in_cnt;                 // [ntiles] incoming particles (counted by the leaver detection)
-    int * stage_off;              // [ntiles] staging offsets (exclusive scan of in_cnt)
-    int * stage_cnt;              // [ntiles] staging fill counters
-    int * new_off; int * new_cap; int * new_np;  // [ntiles] repack layout
+    int * aux; int * aux2;        // [max_part] empty-slot / stayer lists, at off[t]+k
+    int * cnt;                    // [9 ntiles] leavers per tile and direction (particle kernel)
+    int * base;                   // [9 ntiles] first incoming rank per direction (sort check)
+    int * in_cnt;                 // [ntiles] incoming particles (sort check)
+    int * hs;                     // [ntiles] stayers moved down inside the tile (sort)
+    int * overflow;               // [1] a tile's new count exceeds its slot (sort check)
+    int * stage_cnt;              // [ntiles] repack fill counters
+    int * new_off; int * new_cap; int * new_np;  // [ntiles] new counts, repack layout
     int * extra;                  // [ntiles] room to reserve for injection (or nullptr)
-    int * mode;                   // [1] 0 = in-place sort, 1 = repack
+    int * mode;                   // [1] 0 = in-place sort, 1 = repack, 2 = no room
     double * energy;              // [ntiles*nchunk] per work-item kinetic energy sums
     unsigned long long * nmove;   // [0] pushes counter, [1] repacks of the tile slots
     float alpha;                  // 0.5*dt/m_q (species.cpp:2305)
@@ -78,6 +80,8 @@ struct SpDev {
     int perx, pery;               // particle periodic flags
     int bc[4];                    // species::bc
     int min_slack;                // minimum free slots per tile after a repack
+    int sw_every;                 // steps between sorted write-backs of the particle kernel (0: never)
+    int * sw_ctr;                 // [1] steps since the last one (advanced by the sort)
     float jscale;                 // fixed-point tile current: 2^k with |q| * jscale < 2^30
     double jscale_inv;            // 1 / jscale
 };
@@ -107,6 +111,18 @@ __device__ __forceinline__ void mbar_arrive_expect_tx( uint64_t * bar, uint32_t 
                   :: "r"( smem_u32( bar ) ), "r"( bytes ) : "memory" );
 }
 
+// Non-blocking test of an mbarrier phase.
+__device__ __forceinline__ bool mbar_test_wait_parity( uint64_t * bar, uint32_t parity ) {
+    uint32_t ok;
+    asm volatile( "{\n\t.reg .pred p;\n\t"
+                  "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                  "selp.u32 %0, 1, 0, p;\n\t}"
+                  : "=r"( ok ) : "r"( smem_u32( bar ) ), "r"( parity ) : "memory" );
+    return ok != 0;
+}
+
+// Test of an mbarrier phase that may suspend the thread for a while (a
+// hardware-chosen time) before it reports the phase incomplete.
 __device__ __forceinline__ bool mbar_try_wait_parity( uint64_t * bar, uint32_t parity ) {
     uint32_t ok;
     asm volatile( "{\n\t.reg .pred p;\n\t"
@@ -153,11 +169,13 @@ __device__ __forceinline__ void bulk_wait_all() {
 constexpr int WAIT_LIMIT_DEFAULT = 1 << 22;
 
 // Bounded wait on an mbarrier phase.  Gives up after `limit` polls, records
-// ST_WAIT_TIMEOUT (when status is given) and returns false; never traps.
+// ST_WAIT_TIMEOUT (when status is given) and returns false; never traps.  The
+// first poll does not block (so that a limit of 1 tests the phase once), the
+// later ones may.
 __device__ __forceinline__ bool mbar_wait_bounded( uint64_t * bar, uint32_t parity, int * status,
                                                    int limit = WAIT_LIMIT_DEFAULT ) {
     for ( int i = 0; i < limit; i++ ) {
-        if ( mbar_try_wait_parity( bar, parity ) ) return true;
+        if ( i == 0 ? mbar_test_wait_parity( bar, parity ) : mbar_try_wait_parity( bar, parity ) ) return true;
         if ( i > 16 ) __nanosleep( 128 );
     }
     if ( status ) atomicOr( status, ST_WAIT_TIMEOUT );
