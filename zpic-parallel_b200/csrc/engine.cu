@@ -24,11 +24,11 @@
 
 namespace zb {
 struct TileItem { int run; int tile; };
-size_t particle_smem_bytes( int tile_vol, int jacc, int sortw );
+size_t particle_smem_bytes( int tile_vol, int jacc );
 size_t yee_smem_bytes( int tile_vol );
 cudaError_t launch_particles( cudaStream_t, int, int, int, const Item *, int, const SpDev *, const RunDev *, const int *,
                               int, int, int );
-cudaError_t launch_sort( cudaStream_t, const Item *, int, const SpDev *, const int *, int, const RunDev *, int );
+cudaError_t launch_sort( cudaStream_t, const Item *, int, const SpDev *, const int *, int, const RunDev *, int, int * );
 cudaError_t launch_inject( cudaStream_t, int, int, int, int, int, const SpDev *, const RunDev *, const InjRule &, int );
 cudaError_t launch_inj_dyn( cudaStream_t, float *, unsigned *, int, float, float, float, double );
 cudaError_t launch_pack( cudaStream_t, int, int, const SpDev *, const int *, int2 *, float2 *, float * );
@@ -141,7 +141,7 @@ struct HSpecies {
         for ( auto * a : arrs ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
         dfree( d.np ); dfree( d.off ); dfree( d.cap ); dfree( d.nidx ); dfree( d.idx );
         dfree( d.aux ); dfree( d.aux2 ); dfree( d.in_cnt ); dfree( d.stage_cnt );
-        dfree( d.cnt ); dfree( d.base ); dfree( d.hs ); dfree( d.overflow ); dfree( d.sw_ctr );
+        dfree( d.cnt ); dfree( d.base ); dfree( d.hs ); dfree( d.overflow );
         dfree( d.new_off ); dfree( d.new_cap ); dfree( d.new_np ); dfree( d.extra ); dfree( d.mode );
         dfree( d.energy ); dfree( d.nmove ); dfree( inj_dyn ); dfree( mw_nmove_d );
     }
@@ -167,6 +167,7 @@ struct Plan {
     Item * k1_items_d[2] = { nullptr, nullptr }; int n_k1[2] = { 0, 0 };   // boris, euler
     Item * sort_items_d = nullptr; int n_sort = 0;
     int * splist_d = nullptr; int n_sp = 0;
+    int * rlist_d = nullptr;        // [1 + n_sp] species repacking in the current sort (count, then indices)
     // the same work lists grouped per species (fine-grained species calls)
     Item * spk1_d = nullptr;
     std::vector<int> sp_k1_off, sp_k1_n, sp_sort_off, sp_sort_n;
@@ -210,7 +211,7 @@ struct Plan {
         for ( auto & g : mw_graphs ) cudaGraphExecDestroy( g.second.first );
         mw_graphs.clear();
         dfree( runs_d ); dfree( sps_d ); dfree( k1_items_d[0] ); dfree( k1_items_d[1] );
-        dfree( sort_items_d ); dfree( splist_d ); dfree( tile_items_d ); dfree( spk1_d );
+        dfree( sort_items_d ); dfree( splist_d ); dfree( rlist_d ); dfree( tile_items_d ); dfree( spk1_d );
         built = false;
     }
 };
@@ -368,7 +369,7 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
         P.max_guard = std::max( P.max_guard, s->run.extx * s->run.exty - s->run.nxx * s->run.nxy );
         P.max_tile_cells = std::max( P.max_tile_cells, s->run.nxx * s->run.nxy );
         // a batch reorders as often as its most frequent run asks
-        if ( s->reorder_every > 0 && !( s->nxx == 16 && s->nxy == 16 ) )
+        if ( s->reorder_every > 0 )
             P.reorder_every = P.reorder_every > 0 ? std::min( P.reorder_every, s->reorder_every ) : s->reorder_every;
         // one accumulation mode per plan: the runs' own when they agree
         P.jacc = ( P.jacc < 0 || P.jacc == s->jacc ) ? s->jacc : 2;
@@ -385,9 +386,6 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
             HSpecies * sp = s->species[k];
             SpDev d = sp->d;
             if ( batch_chunks ) { d.nchunk = batch_chunks; d.chunk_target = 0; }
-            // in-tile order restored by the particle kernel's sorted write-back
-            // (16x16 tiles), by the reorder kernel otherwise
-            d.sw_every = P.tile_n == 16 ? s->reorder_every : 0;
             d.run = (int) r;
             const int gi = (int) P.sps_h.size();
             P.sps_h.push_back( d );
@@ -410,6 +408,8 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
     TRY( dalloc( &P.runs_d, runs.size() ) );
     TRY( dalloc( &P.sps_d, P.sps_h.size() ) );
     TRY( dalloc( &P.splist_d, splist.size() ) );
+    TRY( dalloc( &P.rlist_d, splist.size() + 1 ) );
+    CK( cudaMemset( P.rlist_d, 0, ( splist.size() + 1 ) * sizeof( int ) ) );
     TRY( dalloc( &P.tile_items_d, tiles.size() ) );
     TRY( dalloc( &P.sort_items_d, sort_items.size() ) );
     CK( cudaStreamCreateWithFlags( &P.side, cudaStreamNonBlocking ) );
@@ -507,7 +507,7 @@ static int run_particles( Plan & P, cudaStream_t st, int push, int move, const i
 static int run_sort( Plan & P, cudaStream_t st, int use_extra ) {
     if ( P.n_sp == 0 ) return ZPIC_OK;
     PhaseScope ps( prof_sim( P ), st, PH_SORT, 4 );
-    DEV( launch_sort( st, P.sort_items_d, P.n_sort, P.sps_d, P.splist_d, P.n_sp, P.runs_d, use_extra ) );
+    DEV( launch_sort( st, P.sort_items_d, P.n_sort, P.sps_d, P.splist_d, P.n_sp, P.runs_d, use_extra, P.rlist_d ) );
     return ZPIC_OK;
 }
 
@@ -880,8 +880,7 @@ static int species_alloc( zpic_sim * s, HSpecies * sp, uint64_t max_part ) {
     TRY( dalloc( &d.idx, max_part ) ); TRY( dalloc( &d.aux, max_part ) ); TRY( dalloc( &d.aux2, max_part ) );
     TRY( dalloc( &d.in_cnt, nt ) ); TRY( dalloc( &d.stage_cnt, nt ) );
     TRY( dalloc( &d.cnt, 9 * (size_t) nt ) ); TRY( dalloc( &d.base, 9 * (size_t) nt ) );
-    TRY( dalloc( &d.hs, nt ) ); TRY( dalloc( &d.overflow, 1 ) ); TRY( dalloc( &d.sw_ctr, 1 ) );
-    CK( cudaMemset( d.sw_ctr, 0, sizeof( int ) ) );
+    TRY( dalloc( &d.hs, nt ) ); TRY( dalloc( &d.overflow, 1 ) );
     CK( cudaMemset( d.cnt, 0, 9 * (size_t) nt * sizeof( int ) ) );
     CK( cudaMemset( d.overflow, 0, sizeof( int ) ) );
     TRY( dalloc( &d.new_off, nt ) ); TRY( dalloc( &d.new_cap, nt ) ); TRY( dalloc( &d.new_np, nt ) );
@@ -1058,7 +1057,7 @@ static int species_sort( zpic_sim * s, int sp, int use_extra ) {
     {
         PhaseScope ps( s, s->stream, PH_SORT, 4 );
         DEV( launch_sort( s->stream, P.sort_items_d + P.sp_sort_off[sp], P.sp_sort_n[sp], P.sps_d,
-                         P.splist_d + sp, 1, P.runs_d, use_extra ) );
+                         P.splist_d + sp, 1, P.runs_d, use_extra, P.rlist_d ) );
     }
     h->sort_pending = false;
     h->counters_dirty = false;
@@ -1197,7 +1196,7 @@ int zpic_b200_sim_create( uint32_t ntx, uint32_t nty, uint32_t nxx, uint32_t nxy
     {
         // every tile kernel stages whole tiles in shared memory (227 KB per block)
         const int tv = roundup4( ( nxx + 3 ) * ( nxy + 3 ) );
-        const size_t need = std::max( particle_smem_bytes( tv, 1, nxx == 16 && nxy == 16 ), yee_smem_bytes( tv ) );
+        const size_t need = std::max( particle_smem_bytes( tv, 1 ), yee_smem_bytes( tv ) );
         if ( nxx > 1024 || nxy > 1024 || need > 227 * 1024 )
             return fail( ZPIC_E_INVALID, "tile too large: its field tiles do not fit in shared memory" );
     }

@@ -16,9 +16,11 @@ namespace zb {
 // Per-particle physics
 // ---------------------------------------------------------------------------
 
-// 1 / Lorentz gamma (species.cpp:22-26)
+// 1 / Lorentz gamma (species.cpp:22-26).  1 / s rounded once is the
+// correctly rounded reciprocal of s, so the reciprocal instruction gives the
+// reference's quotient bit for bit.
 __device__ __forceinline__ float rgamma( float ux, float uy, float uz ) {
-    return 1.0f / sqrtf( __fmaf_rn( uz, uz, __fmaf_rn( uy, uy, __fmaf_rn( ux, ux, 1.0f ) ) ) );
+    return __frcp_rn( sqrtf( __fmaf_rn( uz, uz, __fmaf_rn( uy, uy, __fmaf_rn( ux, ux, 1.0f ) ) ) ) );
 }
 
 // Linear interpolation of the staggered Yee fields (species.cpp:43-92).
@@ -69,7 +71,8 @@ __device__ __forceinline__ void dudt_boris( float alpha, float ex, float ey, flo
     vy = __fmaf_rn( -bz, utx, vy );
     vz = __fmaf_rn( -bx, uty, vz );
     {
-        const float otsq = 2.0f / __fmaf_rn( bz, bz, __fmaf_rn( by, by, __fmaf_rn( bx, bx, 1.0f ) ) );
+        // 2 / d (d >= 1): doubling is exact, so 2 * RN(1/d) = RN(2/d) bit for bit
+        const float otsq = 2.0f * __frcp_rn( __fmaf_rn( bz, bz, __fmaf_rn( by, by, __fmaf_rn( bx, bx, 1.0f ) ) ) );
         bx *= otsq; by *= otsq; bz *= otsq;
     }
     utx = __fmaf_rn( bz, vy, utx );
@@ -345,22 +348,11 @@ __device__ __noinline__ void jfix_flush( int * acc, int n, float * __restrict__ 
 // TN > 0 fixes square TN x TN tiles at compile time, so every shared-memory
 // offset of the interpolation and deposit stencils is an immediate; TN = 0
 // reads the tile shape from the run descriptor.
-//
-// SORTW (16x16 tiles, push + move + deposit): on the steps the species' sort
-// counter selects (every S.sw_every steps), each block of 512 particles is
-// written back sorted by its new cell (leavers last), through a
-// shared-memory counting sort.  Particles keep their slot while they drift
-// between the cells of their tile, so the 32 lanes of a warp end up in random
-// cells and the shared-memory field gathers and current atomics meet ~3.3-way
-// bank conflicts; sorted blocks put a warp's lanes on ~16 consecutive cells
-// again (distinct banks, pairs of lanes on one address).
-template < int PUSH, int MOVE, bool DETECT, typename JT = float, int TN = 0, bool SORTW = false >
+template < int PUSH, int MOVE, bool DETECT, typename JT = float, int TN = 0 >
 __global__ void __launch_bounds__( PK_THREADS, 4 )
 k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
              const RunDev * __restrict__ runs, const int * __restrict__ shifts )
 {
-    static_assert( !SORTW || ( TN == 16 && PUSH && MOVE == 2 && PK_PPT * PK_THREADS == 2 * TN * TN ),
-                   "sorted write-back: 16x16 tiles, full step, 512-particle blocks" );
     extern __shared__ __align__( 16 ) unsigned char smem_raw[];
     const Item it = items[ blockIdx.x ];
     const SpDev & S = sps[ it.sp ];
@@ -379,11 +371,6 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     uint64_t * bar = reinterpret_cast<uint64_t *>( sJ + 3 * tv * JW );
     double * sred = reinterpret_cast<double *>( bar + 1 );
     CrossQueue * xq = reinterpret_cast<CrossQueue *>( sred + PK_THREADS / 32 );
-    // sorted write-back: staging of one block (SoA) and the bucket counts
-    constexpr int SWN = PK_PPT * PK_THREADS;
-    uint32_t * st_c = reinterpret_cast<uint32_t *>( xq + PK_THREADS / 32 );
-    float * st_f = reinterpret_cast<float *>( st_c + SWN );
-    int * hist = reinterpret_cast<int *>( st_f + 5 * SWN );
 
     const int np = S.np[ t ];
     const int off = S.off[ t ];
@@ -468,8 +455,6 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
     const unsigned lt_mask = ( 1u << lane ) - 1u;
     CrossQueue & Q = xq[ threadIdx.x >> 5 ];
     int qh = 0, qt = 0;                         // warp-uniform ring head / tail
-    // sorted write-back on this step (CTA-uniform)
-    const bool sw = SORTW && S.sw_every > 0 && *S.sw_ctr == 0;
 
     // Groups of FLUSH_PARTICLES: with the fixed-point tile current the
     // accumulators are flushed between groups (at most 3 additions per
@@ -574,62 +559,14 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
                     }
                 }
             }
-            int dst[PK_PPT];
-            if ( SORTW && sw ) {
-                // counting sort of the block by new cell: bucket = cell, TN*TN
-                // for particles outside the tile (leavers, flagged ones)
-                constexpr int NB = TN * TN;
-                int key[PK_PPT], rk[PK_PPT];
-                __syncthreads();                  // the previous block's staging has been read
-                for ( int q = threadIdx.x; q <= NB; q += PK_THREADS ) hist[q] = 0;
-                __syncthreads();
 #pragma unroll
-                for ( int k = 0; k < PK_PPT; k++ ) {
-                    const int i = b0 + k * PK_THREADS + threadIdx.x;
-                    key[k] = -1; rk[k] = 0;
-                    if ( i < end ) {
-                        const int ix = cell_x( c[k] ), iy = cell_y( c[k] );
-                        key[k] = ( ix >= 0 && ix < TN && iy >= 0 && iy < TN ) ? iy * TN + ix : NB;
-                        rk[k] = atomicAdd( &hist[ key[k] ], 1 );
-                    }
-                }
-                __syncthreads();
-                __shared__ long long s_tot;
-                const long long ex = block_exscan< PK_THREADS >( hist[ threadIdx.x ], &s_tot );
-                hist[ threadIdx.x ] = (int) ex;
-                if ( threadIdx.x == 0 ) hist[ NB ] = (int) s_tot;
-                __syncthreads();
-#pragma unroll
-                for ( int k = 0; k < PK_PPT; k++ ) {
-                    dst[k] = k * PK_THREADS + threadIdx.x;
-                    if ( key[k] >= 0 ) {
-                        const int d = hist[ key[k] ] + rk[k];
-                        dst[k] = d;
-                        st_c[d] = c[k];
-                        st_f[d] = x0[k]; st_f[SWN + d] = x1[k];
-                        st_f[2 * SWN + d] = u0[k]; st_f[3 * SWN + d] = u1[k]; st_f[4 * SWN + d] = u2[k];
-                    }
-                }
-                __syncthreads();
-#pragma unroll
-                for ( int k = 0; k < PK_PPT; k++ ) {
-                    const int j = k * PK_THREADS + threadIdx.x, i = b0 + j;
-                    if ( i < end ) {
-                        pc[i] = st_c[j]; pxx[i] = st_f[j]; pxy[i] = st_f[SWN + j];
-                        pux[i] = st_f[2 * SWN + j]; puy[i] = st_f[3 * SWN + j]; puz[i] = st_f[4 * SWN + j];
-                    }
-                }
-            } else {
-#pragma unroll
-                for ( int k = 0; k < PK_PPT; k++ ) {
-                    dst[k] = k * PK_THREADS + threadIdx.x;
-                    const int i = b0 + dst[k];
-                    if ( i < end ) {
-                        if ( MOVE ) { pc[i] = c[k]; pxx[i] = x0[k]; pxy[i] = x1[k]; }
-                        if ( PUSH || rxl || rxu ) pux[i] = u0[k];
-                        if ( PUSH || ryl || ryu ) puy[i] = u1[k];
-                        if ( PUSH ) puz[i] = u2[k];
-                    }
+            for ( int k = 0; k < PK_PPT; k++ ) {
+                const int i = b0 + k * PK_THREADS + threadIdx.x;
+                if ( i < end ) {
+                    if ( MOVE ) { pc[i] = c[k]; pxx[i] = x0[k]; pxy[i] = x1[k]; }
+                    if ( PUSH || rxl || rxu ) pux[i] = u0[k];
+                    if ( PUSH || ryl || ryu ) puy[i] = u1[k];
+                    if ( PUSH ) puz[i] = u2[k];
                 }
             }
 
@@ -654,7 +591,7 @@ k_particles( const Item * __restrict__ items, const SpDev * __restrict__ sps,
 #pragma unroll
                     for ( int k = 0; k < PK_PPT; k++ ) {
                         if ( leave_dir[k] != 4 ) {
-                            const int li = b0 + dst[k];
+                            const int li = b0 + k * PK_THREADS + threadIdx.x;
                             S.idx[ off + pos ] = li;
                             // leaver outbox in buffer B (unused outside a repack),
                             // so that the sort reads the leavers coalesced
@@ -758,9 +695,10 @@ constexpr int CHECK_THREADS = 256;
 // direction d come from the neighbour in the opposite direction 8 - d.
 __global__ void __launch_bounds__( CHECK_THREADS )
 k_sort_check( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps,
-              const RunDev * __restrict__ runs, int use_extra )
+              const RunDev * __restrict__ runs, int use_extra, int * __restrict__ rlist )
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if ( i == 0 ) rlist[0] = 0;                   // the plan lists the species that repack
     if ( i >= nitems ) return;
     const Item it = items[i];
     const SpDev & S = sps[ it.sp ];
@@ -791,17 +729,13 @@ constexpr int PLAN_THREADS = 1024;
 // new total (ST_CAPACITY: the host grows buffers before that can happen).
 __global__ void __launch_bounds__( PLAN_THREADS )
 k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_list,
-             const RunDev * __restrict__ runs, int use_extra )
+             const RunDev * __restrict__ runs, int use_extra, int * __restrict__ rlist )
 {
     const SpDev & S = sps[ species_list[ blockIdx.x ] ];
     const RunDev & R = runs[ S.run ];
     const int over = *S.overflow;
     __syncthreads();
-    // steps until the particle kernel's next sorted write-back
-    if ( threadIdx.x == 0 && S.sw_every > 0 ) {
-        const int c = *S.sw_ctr + 1;
-        *S.sw_ctr = c >= S.sw_every ? 0 : c;
-    }
+
     if ( !over ) {
         if ( threadIdx.x == 0 ) *S.mode = 0;
         return;
@@ -811,14 +745,19 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
     const int per = ( nt + PLAN_THREADS - 1 ) / PLAN_THREADS;
     const int t0 = min( nt, (int) threadIdx.x * per ), t1 = min( nt, t0 + per );
     __shared__ long long s_total;
-    long long need_sum = 0, w_sum = 0;
+    long long need_sum = 0, w_sum = 0, np_sum = 0;
     for ( int t = t0; t < t1; t++ ) {
         const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
         const int need = ( S.new_np[t] + ex + 3 ) & ~3;
         need_sum += need;
         w_sum += need + S.min_slack;
+        np_sum += S.np[t];
         S.stage_cnt[t] = 0;
     }
+    // packed position of each tile's first particle (the repack's index space)
+    long long pk = block_exscan< PLAN_THREADS >( np_sum, &s_total );
+    for ( int t = t0; t < t1; t++ ) { S.hs[t] = (int) pk; pk += S.np[t]; }
+    __syncthreads();
     block_exscan< PLAN_THREADS >( need_sum, &s_total );
     const long long need_total = s_total;
     __syncthreads();
@@ -841,7 +780,11 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
     __syncthreads();
     long long pc = block_exscan< PLAN_THREADS >( cap_sum, &s_total );
     for ( int t = t0; t < t1; t++ ) { S.new_off[t] = (int) pc; pc += S.new_cap[t]; }
-    if ( threadIdx.x == 0 ) { *S.mode = 1; S.nmove[1] += 1; }
+    if ( threadIdx.x == 0 ) {
+        *S.mode = 1;
+        S.nmove[1] += 1;
+        rlist[ 1 + atomicAdd( rlist, 1 ) ] = species_list[ blockIdx.x ];
+    }
 }
 
 __device__ __forceinline__ void copy_particle( const PartArrays & d, size_t di, const PartArrays & s, size_t si ) {
@@ -855,26 +798,31 @@ constexpr int SU = 4;                             // sort entries per lane in fl
 
 // Repack, first half (mode 1): every particle of the species goes to buffer B
 // in the new slot layout -- stayers into their own tile's new slot, leavers
-// into their target's.  The whole grid strides over the particle buffer (a
-// tile's particles are spread over all CTAs, however unevenly the tiles are
-// filled); slots are claimed per destination with one atomic per group of
+// into their target's.  The whole grid strides over the species' particles
+// in packed order (q-th particle: tile t with hs[t] <= q < hs[t] + np[t], the
+// packed offsets the plan wrote into hs), so a tile's particles are spread
+// over all CTAs however unevenly the tiles are filled, and slack is not
+// visited; slots are claimed per destination with one atomic per group of
 // lanes sharing it.
 __device__ void repack_out( const SpDev & S, const RunDev & R ) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = ( 1u << lane ) - 1u;
     const int nt = S.ntiles, ntx = R.ntx, nty = R.nty, nxx = R.nxx, nxy = R.nxy;
-    const long long n = S.max_part;
-    for ( long long p0 = (long long) blockIdx.x * blockDim.x; p0 < n; p0 += (long long) gridDim.x * blockDim.x ) {
-        const long long p = p0 + threadIdx.x;
+    const long long n = (long long) S.hs[ nt - 1 ] + S.np[ nt - 1 ];
+    for ( long long q0 = (long long) blockIdx.x * blockDim.x; q0 < n; q0 += (long long) gridDim.x * blockDim.x ) {
+        const long long q = q0 + threadIdx.x;
         int dest = -1, ix = 0, iy = 0, xc = 0, yc = 0;
-        if ( p < n ) {
-            // tile of slot p: the last tile whose slot starts at or before p
+        long long p = 0;
+        if ( q < n ) {
+            // the last tile whose first packed position is at or before q (a
+            // tile without particles shares its position with the next one)
             int lo = 0, hi = nt - 1;
             while ( lo < hi ) {
                 const int mid = ( lo + hi + 1 ) >> 1;
-                if ( S.off[mid] <= p ) lo = mid; else hi = mid - 1;
+                if ( S.hs[mid] <= q ) lo = mid; else hi = mid - 1;
             }
-            const int t = lo, i = (int) ( p - S.off[t] );
+            const int t = lo, i = (int) ( q - S.hs[t] );
+            p = (long long) S.off[t] + i;
             if ( i >= 0 && i < S.np[t] ) {
                 const uint32_t c = S.A.cell[p];
                 ix = cell_x( c ); iy = cell_y( c );
@@ -926,7 +874,7 @@ __device__ void repack_in( const SpDev & S ) {
 template < int WPT >
 __global__ void __launch_bounds__( SORT_THREADS )
 k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps,
-              const int * __restrict__ species_list, int nspecies, const RunDev * __restrict__ runs )
+              const int * __restrict__ rlist, const RunDev * __restrict__ runs )
 {
     constexpr int TPB = SORT_WARPS / WPT;         // tiles per CTA
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1023,9 +971,10 @@ k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restr
         }
         if ( sub == 0 && lane == 0 ) S.hs[t] = ns;
     }
-    for ( int k = 0; k < nspecies; k++ ) {
-        const SpDev & S = sps[ species_list[k] ];
-        if ( *S.mode == 1 ) repack_out( S, runs[ S.run ] );
+    const int nr = rlist[0];
+    for ( int k = 0; k < nr; k++ ) {
+        const SpDev & S = sps[ rlist[ 1 + k ] ];
+        repack_out( S, runs[ S.run ] );
     }
 }
 
@@ -1038,7 +987,7 @@ k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restr
 template < int WPT >
 __global__ void __launch_bounds__( SORT_THREADS )
 k_sort_scatter( const Item * __restrict__ items, int nitems, const SpDev * __restrict__ sps,
-                const int * __restrict__ species_list, int nspecies, const RunDev * __restrict__ runs )
+                const int * __restrict__ rlist, const RunDev * __restrict__ runs )
 {
     constexpr int TPB = SORT_WARPS / WPT;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1124,10 +1073,8 @@ k_sort_scatter( const Item * __restrict__ items, int nitems, const SpDev * __res
         else { S.np[t] = S.new_np[t]; S.off[t] = S.new_off[t]; S.cap[t] = S.new_cap[t]; }
         S.nidx[t] = 0;
     }
-    for ( int k = 0; k < nspecies; k++ ) {
-        const SpDev & S = sps[ species_list[k] ];
-        if ( *S.mode == 1 ) repack_in( S );
-    }
+    const int nr = rlist[0];
+    for ( int k = 0; k < nr; k++ ) repack_in( sps[ rlist[ 1 + k ] ] );
 }
 
 // ---------------------------------------------------------------------------
@@ -1565,22 +1512,19 @@ k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, cons
 // ---------------------------------------------------------------------------
 namespace zb {
 
-// Shared memory of the particle kernel; sortw adds the staging of the sorted
-// write-back (one 512-particle block, SoA) and its 257 bucket counts.
-size_t particle_smem_bytes( int tile_vol, int jacc, int sortw ) {
+size_t particle_smem_bytes( int tile_vol, int jacc ) {
     return (size_t) ( jacc ? 12 : 9 ) * tile_vol * sizeof( float ) + 8 + ( PK_THREADS / 32 ) * sizeof( double ) +
-           ( PK_THREADS / 32 ) * sizeof( CrossQueue ) +
-           ( sortw ? (size_t) PK_PPT * PK_THREADS * 6 * 4 + 260 * 4 : 0 );
+           ( PK_THREADS / 32 ) * sizeof( CrossQueue );
 }
 
 typedef void ( *pk_fn )( const Item *, const SpDev *, const RunDev *, const int * );
 
 static pk_fn pick_particle_kernel( int push, int move, int detect, int jacc, int tile_n ) {
     if ( tile_n == 16 && move == 2 && detect && ( push == 1 || push == 2 ) ) {
-        if ( jacc == 0 ) return push == 1 ? k_particles< 1, 2, true, float, 16, true > : k_particles< 2, 2, true, float, 16, true >;
-        if ( jacc == 1 ) return push == 1 ? k_particles< 1, 2, true, double, 16, true > : k_particles< 2, 2, true, double, 16, true >;
-        return push == 1 ? k_particles< 1, 2, true, int, 16, true >
-                         : k_particles< 2, 2, true, int, 16, true >;
+        if ( jacc == 0 ) return push == 1 ? k_particles< 1, 2, true, float, 16 > : k_particles< 2, 2, true, float, 16 >;
+        if ( jacc == 1 ) return push == 1 ? k_particles< 1, 2, true, double, 16 > : k_particles< 2, 2, true, double, 16 >;
+        return push == 1 ? k_particles< 1, 2, true, int, 16 >
+                         : k_particles< 2, 2, true, int, 16 >;
     }
     if ( jacc == 1 && move == 2 ) {
 #define PKD( P, M, D ) if ( push == P && move == M && detect == D ) return k_particles< P, M, D, double >;
@@ -1609,8 +1553,7 @@ cudaError_t launch_particles( cudaStream_t st, int push, int move, int detect, c
     if ( move != 2 ) jacc = 0;
     pk_fn f = pick_particle_kernel( push, move, detect, jacc, tile_n );
     if ( !f ) return cudaErrorInvalidValue;
-    const bool sortw = tile_n == 16 && move == 2 && detect && ( push == 1 || push == 2 );
-    const size_t smem = particle_smem_bytes( max_tile_vol, jacc, sortw );
+    const size_t smem = particle_smem_bytes( max_tile_vol, jacc );
     if ( smem > 48 * 1024 )
         cudaFuncSetAttribute( (const void *) f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
     if ( nitems <= 0 ) return cudaSuccess;
@@ -1619,14 +1562,14 @@ cudaError_t launch_particles( cudaStream_t st, int push, int move, int detect, c
 }
 
 cudaError_t launch_sort( cudaStream_t st, const Item * items, int nitems, const SpDev * sps,
-                         const int * species_list, int nspecies, const RunDev * runs, int use_extra ) {
+                         const int * species_list, int nspecies, const RunDev * runs, int use_extra, int * rlist ) {
     if ( nitems <= 0 ) return cudaSuccess;
     int dev = 0, sms = 148;
     cudaGetDevice( &dev );
     cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
     k_sort_check<<< ( nitems + CHECK_THREADS - 1 ) / CHECK_THREADS, CHECK_THREADS, 0, st >>>( items, nitems, sps, runs,
-                                                                                         use_extra );
-    k_sort_plan<<< nspecies, PLAN_THREADS, 0, st >>>( sps, species_list, runs, use_extra );
+                                                                                         use_extra, rlist );
+    k_sort_plan<<< nspecies, PLAN_THREADS, 0, st >>>( sps, species_list, runs, use_extra, rlist );
     // a warp per tile, unless the tiles are too few to occupy the GPU's SMs
     // (then they are large, and get a CTA each); the grid covers the GPU at
     // least once for the repack's grid-stride loops
@@ -1634,11 +1577,11 @@ cudaError_t launch_sort( cudaStream_t st, const Item * items, int nitems, const 
     const int tpb = wide ? 1 : SORT_WARPS;
     const int nb = std::max( ( nitems + tpb - 1 ) / tpb, 4 * sms );
     if ( wide ) {
-        k_sort_local< SORT_WARPS ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, species_list, nspecies, runs );
-        k_sort_scatter< SORT_WARPS ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, species_list, nspecies, runs );
+        k_sort_local< SORT_WARPS ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, rlist, runs );
+        k_sort_scatter< SORT_WARPS ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, rlist, runs );
     } else {
-        k_sort_local< 1 ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, species_list, nspecies, runs );
-        k_sort_scatter< 1 ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, species_list, nspecies, runs );
+        k_sort_local< 1 ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, rlist, runs );
+        k_sort_scatter< 1 ><<< nb, SORT_THREADS, 0, st >>>( items, nitems, sps, rlist, runs );
     }
     return cudaGetLastError();
 }

@@ -80,8 +80,6 @@ struct SpDev {
     int perx, pery;               // particle periodic flags
     int bc[4];                    // species::bc
     int min_slack;                // minimum free slots per tile after a repack
-    int sw_every;                 // steps between sorted write-backs of the particle kernel (0: never)
-    int * sw_ctr;                 // [1] steps since the last one (advanced by the sort)
     float jscale;                 // fixed-point tile current: 2^k with |q| * jscale < 2^30
     double jscale_inv;            // 1 / jscale
 };
