@@ -141,7 +141,7 @@ struct HSpecies {
         for ( auto * a : arrs ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
         dfree( d.np ); dfree( d.off ); dfree( d.cap ); dfree( d.nidx ); dfree( d.idx );
         dfree( d.aux ); dfree( d.aux2 ); dfree( d.in_cnt ); dfree( d.stage_cnt );
-        dfree( d.cnt ); dfree( d.base ); dfree( d.hs ); dfree( d.overflow );
+        dfree( d.cnt ); dfree( d.base ); dfree( d.hs ); dfree( d.pk ); dfree( d.overflow );
         dfree( d.new_off ); dfree( d.new_cap ); dfree( d.new_np ); dfree( d.extra ); dfree( d.mode );
         dfree( d.energy ); dfree( d.nmove ); dfree( inj_dyn ); dfree( mw_nmove_d );
     }
@@ -880,7 +880,7 @@ static int species_alloc( zpic_sim * s, HSpecies * sp, uint64_t max_part ) {
     TRY( dalloc( &d.idx, max_part ) ); TRY( dalloc( &d.aux, max_part ) ); TRY( dalloc( &d.aux2, max_part ) );
     TRY( dalloc( &d.in_cnt, nt ) ); TRY( dalloc( &d.stage_cnt, nt ) );
     TRY( dalloc( &d.cnt, 9 * (size_t) nt ) ); TRY( dalloc( &d.base, 9 * (size_t) nt ) );
-    TRY( dalloc( &d.hs, nt ) ); TRY( dalloc( &d.overflow, 1 ) );
+    TRY( dalloc( &d.hs, nt ) ); TRY( dalloc( &d.pk, nt ) ); TRY( dalloc( &d.overflow, 1 ) );
     CK( cudaMemset( d.cnt, 0, 9 * (size_t) nt * sizeof( int ) ) );
     CK( cudaMemset( d.overflow, 0, sizeof( int ) ) );
     TRY( dalloc( &d.new_off, nt ) ); TRY( dalloc( &d.new_cap, nt ) ); TRY( dalloc( &d.new_np, nt ) );

@@ -768,7 +768,7 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
         if ( threadIdx.x == 0 ) { *S.mode = 2; atomicOr( R.status, ST_CAPACITY ); }
         return;
     }
-    long long cap_sum = 0;
+    long long cap_sum = 0, nnp_sum = 0;
     for ( int t = t0; t < t1; t++ ) {
         const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
         const int need = ( S.new_np[t] + ex + 3 ) & ~3;
@@ -776,10 +776,14 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
         const int c = need + (int) ( slack & ~3LL );
         S.new_cap[t] = c;
         cap_sum += c;
+        nnp_sum += S.new_np[t];
     }
     __syncthreads();
     long long pc = block_exscan< PLAN_THREADS >( cap_sum, &s_total );
     for ( int t = t0; t < t1; t++ ) { S.new_off[t] = (int) pc; pc += S.new_cap[t]; }
+    __syncthreads();
+    long long pn = block_exscan< PLAN_THREADS >( nnp_sum, &s_total );
+    for ( int t = t0; t < t1; t++ ) { S.pk[t] = (int) pn; pn += S.new_np[t]; }
     if ( threadIdx.x == 0 ) {
         *S.mode = 1;
         S.nmove[1] += 1;
@@ -804,7 +808,7 @@ constexpr int SU = 4;                             // sort entries per lane in fl
 // over all CTAs however unevenly the tiles are filled, and slack is not
 // visited; slots are claimed per destination with one atomic per group of
 // lanes sharing it.
-__device__ void repack_out( const SpDev & S, const RunDev & R ) {
+__device__ __noinline__ void repack_out( const SpDev & S, const RunDev & R ) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = ( 1u << lane ) - 1u;
     const int nt = S.ntiles, ntx = R.ntx, nty = R.nty, nxx = R.nxx, nxy = R.nxy;
@@ -844,22 +848,22 @@ __device__ void repack_out( const SpDev & S, const RunDev & R ) {
     }
 }
 
-// Repack, second half: B -> A over the whole buffer (slack included),
-// 16-byte vectors (the arrays are cudaMalloc'd, 256-byte aligned); the last
-// max_part % 4 entries are copied singly.
-__device__ __forceinline__ void copy_vec( void * dst, const void * src, long long i ) {
-    reinterpret_cast<uint4 *>( dst )[i] = reinterpret_cast<const uint4 *>( src )[i];
-}
-
-__device__ void repack_in( const SpDev & S ) {
-    const long long n = S.max_part, n4 = n / 4;
+// Repack, second half: B -> A, the particles of the new layout only (its
+// slack is not copied), by packed index over the new counts (pk, the plan's
+// prefix of new_np), so consecutive threads copy consecutive slots.
+__device__ __noinline__ void repack_in( const SpDev & S ) {
+    const int nt = S.ntiles;
+    const long long n = (long long) S.pk[ nt - 1 ] + S.new_np[ nt - 1 ];
     const long long stride = (long long) gridDim.x * blockDim.x;
-    for ( long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride ) {
-        copy_vec( S.A.cell, S.B.cell, i ); copy_vec( S.A.xx, S.B.xx, i ); copy_vec( S.A.xy, S.B.xy, i );
-        copy_vec( S.A.ux, S.B.ux, i );     copy_vec( S.A.uy, S.B.uy, i ); copy_vec( S.A.uz, S.B.uz, i );
+    for ( long long q = (long long) blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride ) {
+        int lo = 0, hi = nt - 1;
+        while ( lo < hi ) {
+            const int mid = ( lo + hi + 1 ) >> 1;
+            if ( S.pk[mid] <= q ) lo = mid; else hi = mid - 1;
+        }
+        const size_t p = (size_t) S.new_off[lo] + ( q - S.pk[lo] );
+        copy_particle( S.A, p, S.B, p );
     }
-    for ( long long p = 4 * n4 + blockIdx.x * (long long) blockDim.x + threadIdx.x; p < n; p += stride )
-        copy_particle( S.A, (size_t) p, S.B, (size_t) p );
 }
 
 // Per tile (WPT warps per tile; 1 when there are many tiles, a whole CTA when
@@ -1030,36 +1034,56 @@ k_sort_scatter( const Item * __restrict__ items, int nitems, const SpDev * __res
         const RunDev & R = runs[ S.run ];
         const int t = it.tile, nxx = R.nxx, nxy = R.nxy;
         const int nl = S.nidx[t], off = S.off[t];
-        for ( int k0 = sub * 32; k0 < nl; k0 += WPT * 32 ) {
-            const int k = k0 + lane;
-            const bool in = k < nl;
-            const size_t g = (size_t) off + k;
-            uint32_t c = 0; float xx = 0.f, xy = 0.f, ux = 0.f, uy = 0.f, uz = 0.f;
-            if ( in ) { c = S.B.cell[g]; xx = S.B.xx[g]; xy = S.B.xy[g]; ux = S.B.ux[g]; uy = S.B.uy[g]; uz = S.B.uz[g]; }
-            const int ix = cell_x( c ), iy = cell_y( c );
-            const int xc = ( ix >= nxx ) - ( ix < 0 ), yc = ( iy >= nxy ) - ( iy < 0 );
-            const int d = in ? ( yc + 1 ) * 3 + xc + 1 : 9;
-            const unsigned peers = __match_any_sync( 0xffffffffu, d );
-            const int leader = __ffs( peers ) - 1;
-            int b = 0;
-            if ( d < 9 && lane == leader ) b = atomicAdd( &s_rank[tib][d], __popc( peers ) );
-            b = __shfl_sync( peers, b, leader );
-            if ( d < 9 && d != 4 ) {
-                const int a = s_aux[tib][d];
-                if ( a >= 0 ) {
+        // SU groups of 32 leavers in flight: their outbox loads, then their
+        // slot lookups, then their stores
+        for ( int k0 = sub * 32 * SU; k0 < nl; k0 += WPT * 32 * SU ) {
+            uint32_t c[SU]; float xx[SU], xy[SU], ux[SU], uy[SU], uz[SU];
+#pragma unroll
+            for ( int u = 0; u < SU; u++ ) {
+                const int k = k0 + u * 32 + lane;
+                const size_t g = (size_t) off + k;
+                c[u] = 0x80008000u;                   // (-32768, -32768): no leaver
+                xx[u] = xy[u] = ux[u] = uy[u] = uz[u] = 0.f;
+                if ( k < nl ) {
+                    c[u] = S.B.cell[g]; xx[u] = S.B.xx[g]; xy[u] = S.B.xy[g];
+                    ux[u] = S.B.ux[g]; uy[u] = S.B.uy[g]; uz[u] = S.B.uz[g];
+                }
+            }
+            int slot[SU], dir[SU];
+#pragma unroll
+            for ( int u = 0; u < SU; u++ ) {
+                const int k = k0 + u * 32 + lane;
+                const int ix = cell_x( c[u] ), iy = cell_y( c[u] );
+                const int xc = ( ix >= nxx ) - ( ix < 0 ), yc = ( iy >= nxy ) - ( iy < 0 );
+                const int d = k < nl ? ( yc + 1 ) * 3 + xc + 1 : 9;
+                const unsigned peers = __match_any_sync( 0xffffffffu, d );
+                const int leader = __ffs( peers ) - 1;
+                int b = 0;
+                if ( d < 9 && lane == leader ) b = atomicAdd( &s_rank[tib][d], __popc( peers ) );
+                b = __shfl_sync( peers, b, leader );
+                dir[u] = d;
+                slot[u] = -2;                          // -2: nothing to write
+                if ( d < 9 && d != 4 && s_aux[tib][d] >= 0 ) {
                     // list entry and slot both below the target's new count
                     // (anything else means inconsistent counts: reported, the
                     // particle is not written)
-                    const int r = a + b + __popc( peers & lt ), nnt = s_cap[tib][d];
-                    const int slot = r < nnt ? S.aux[ (size_t) s_off[tib][d] + r ] : -1;
-                    if ( slot >= 0 && slot < nnt ) {
-                        const size_t p = (size_t) s_off[tib][d] + slot;
-                        S.A.cell[p] = pack_cell( ix - xc * nxx, iy - yc * nxy );
-                        S.A.xx[p] = xx; S.A.xy[p] = xy;
-                        S.A.ux[p] = ux; S.A.uy[p] = uy; S.A.uz[p] = uz;
-                    } else {
-                        atomicOr( R.status, ST_BAD_CELL );
-                    }
+                    const int r = s_aux[tib][d] + b + __popc( peers & lt );
+                    slot[u] = r < s_cap[tib][d] ? S.aux[ (size_t) s_off[tib][d] + r ] : -1;
+                }
+            }
+#pragma unroll
+            for ( int u = 0; u < SU; u++ ) {
+                if ( slot[u] == -2 ) continue;
+                const int d = dir[u];
+                if ( slot[u] >= 0 && slot[u] < s_cap[tib][d] ) {
+                    const int ix = cell_x( c[u] ), iy = cell_y( c[u] );
+                    const int xc = d % 3 - 1, yc = d / 3 - 1;
+                    const size_t p = (size_t) s_off[tib][d] + slot[u];
+                    S.A.cell[p] = pack_cell( ix - xc * nxx, iy - yc * nxy );
+                    S.A.xx[p] = xx[u]; S.A.xy[p] = xy[u];
+                    S.A.ux[p] = ux[u]; S.A.uy[p] = uy[u]; S.A.uz[p] = uz[u];
+                } else {
+                    atomicOr( R.status, ST_BAD_CELL );
                 }
             }
         }

@@ -65,7 +65,9 @@ struct SpDev {
     int * cnt;                    // [9 ntiles] leavers per tile and direction (particle kernel)
     int * base;                   // [9 ntiles] first incoming rank per direction (sort check)
     int * in_cnt;                 // [ntiles] incoming particles (sort check)
-    int * hs;                     // [ntiles] stayers moved down inside the tile (sort)
+    int * hs;                     // [ntiles] stayers moved down inside the tile (sort); in a repack:
+                                  // packed position of each tile's first particle, old layout
+    int * pk;                     // [ntiles] repack: packed position of each tile's first particle, new layout
     int * overflow;               // [1] a tile's new count exceeds its slot (sort check)
     int * stage_cnt;              // [ntiles] repack fill counters
     int * new_off; int * new_cap; int * new_np;  // [ntiles] new counts, repack layout
