@@ -542,6 +542,9 @@ def ensemble_measure(args, world, rank, local, nruns, steps):
     tc = timed(sstreams, concurrent)
     for s in sims:
         s.synchronize()
+    # tile-slot rebuilds over the three timed runs (and warm-ups)
+    repacks = sum(s.repacks(k) for s in sims for k in range(2))
+    relocations = sum(s.relocations(k) for s in sims for k in range(2))
     batch.close()
     for s in sims:
         s.close()
@@ -564,6 +567,7 @@ def ensemble_measure(args, world, rank, local, nruns, steps):
         'gpu_launches': launches,
         'ctas_per_tile': chunks if chunks is not None else 'automatic',
         'setup_s': setup_s,
+        'slot_repacks': repacks, 'tiles_relocated': relocations,
         'clocks': clk.summary(),
     }
 
@@ -641,6 +645,7 @@ def run_lwfa(args, world, rank, local):
             'phase_ms_per_step': phases,
             'host_issue_ms_per_step': host_s / steps * 1e3,
             'setup_s': {'simulation_and_species': t_set1 - t_set0, 'gaussian_laser_on_host': t_set2 - t_set1},
+            'slot_repacks': s.repacks(0), 'tiles_relocated': s.relocations(0),
             'clocks': clk.summary(),
         }))
     s.close()

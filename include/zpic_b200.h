@@ -224,6 +224,9 @@ int zpic_b200_species_np_total( zpic_sim * sim, int32_t sp, uint64_t * np );   /
 /* Times the tile sort had to rebuild the slot layout of this species (a full
  * copy of its particles through the second buffer); no reference counterpart. */
 int zpic_b200_species_repacks( zpic_sim * sim, int32_t sp, uint64_t * repacks );
+/* Tiles that outgrew their slot and were moved into the free pool at the
+ * end of the buffer (instead of a repack); no reference counterpart. */
+int zpic_b200_species_relocations( zpic_sim * sim, int32_t sp, uint64_t * tiles );
 int zpic_b200_species_np_max_tile( zpic_sim * sim, int32_t sp, uint32_t * np );/* Species::np_max_tile */
 /* Particle-buffer capacity (the public Particles::max_part, particles.h:82-105).
  * It grows, as the reference's does in its sort (particles.cpp:863-888), when

@@ -57,17 +57,24 @@ def test_full_size_invariants(big):
     assert big.np_max_tile(0) == npt.max()
 
 
-def test_repack_path_free_streaming():
-    """A drifting slab fills empty tiles beyond their spare room, forcing the
-    sort's repack path many times; free streaming keeps every particle
-    bit-exact, so tile counts and multisets must match the oracle exactly."""
+@pytest.mark.parametrize('capacity', [None, 0.3])
+def test_relocation_and_repack_free_streaming(capacity):
+    """A drifting slab fills empty tiles beyond their spare room: such tiles
+    move into the free pool at the end of the buffer (relocation), and with
+    little capacity the pool runs out and the whole layout is rebuilt
+    (repack).  Free streaming keeps every particle bit-exact, so tile counts
+    and multisets must match the oracle exactly."""
     geom = ((8, 4), (16, 16), (12.8, 6.4), 0.07)
 
     def setup(s):
         s.add_species(-1.0, (4, 4), density=('slab', 1.0, 0.5, 3.0, 0),
                       udist=('thermal', (0.05, 0.05, 0.05), (0.9, 0.0, 0.0)))
         return s
-    o, g = setup(OracleSim(*geom)), setup(zb.Simulation(*geom))
+    o = setup(OracleSim(*geom))
+    g = zb.Simulation(*geom)
+    if capacity is not None:
+        g.set_option('capacity_factor', capacity)
+    setup(g)
     occupied0 = set(np.nonzero(o.tiles(0)[0])[0])
     for n in range(1, 121):
         o.species_advance_free(0)
@@ -76,6 +83,9 @@ def test_repack_path_free_streaming():
             assert same_multisets(o.particles(0), g.particles(0)), 'step %d' % n
     # the slab moved into tiles that were empty at the start
     assert set(np.nonzero(o.tiles(0)[0])[0]) - occupied0
+    assert g.relocations(0) > 0
+    if capacity is not None:
+        assert g.repacks(0) > 0
 
 
 @pytest.mark.parametrize('ntiles,bc', [

@@ -129,6 +129,7 @@ struct HSpecies {
     uint32_t max_part = 0;
     uint64_t np_bound = 0;    // upper bound of the particle count (capacity checks)
     int grows = 0;            // particle-buffer growths so far
+    int pool_h = 0;           // host copy of the pool start at the last upload (copy source)
     SpDev d{};                // descriptor (device pointers)
     bool sort_pending = false;
     bool counters_dirty = false;
@@ -141,7 +142,7 @@ struct HSpecies {
         for ( auto * a : arrs ) { dfree( a->cell ); dfree( a->xx ); dfree( a->xy ); dfree( a->ux ); dfree( a->uy ); dfree( a->uz ); }
         dfree( d.np ); dfree( d.off ); dfree( d.cap ); dfree( d.nidx ); dfree( d.idx );
         dfree( d.aux ); dfree( d.aux2 ); dfree( d.in_cnt ); dfree( d.stage_cnt );
-        dfree( d.cnt ); dfree( d.base ); dfree( d.hs ); dfree( d.pk ); dfree( d.overflow );
+        dfree( d.cnt ); dfree( d.base ); dfree( d.hs ); dfree( d.overflow ); dfree( d.reloc ); dfree( d.pool );
         dfree( d.new_off ); dfree( d.new_cap ); dfree( d.new_np ); dfree( d.extra ); dfree( d.mode );
         dfree( d.energy ); dfree( d.nmove ); dfree( inj_dyn ); dfree( mw_nmove_d );
     }
@@ -250,6 +251,8 @@ struct zpic_sim {
     int reorder_every = REORDER_DEFAULT;
     int chunks_opt = 0;
     int jacc = 2;                   // fixed-point tile current (option "jacc")
+    double pool_frac = 0.5;         // share of free particle capacity kept as the pool (option "pool_fraction")
+    double reloc_room = 1.0;        // room for a relocated tile, share of its count (option "relocation_room")
     double capacity_factor = 1.2;   // initial particle capacity per cell and ppc (option "capacity_factor";
                                     // the reference's max_part = 1.2 cells ppc, species.cpp:1752)
     int profile = 0;                // 1: per-phase events, steps issued eagerly; 2: the same inside CUDA graphs
@@ -750,15 +753,17 @@ static int plan_advance( Plan & P, cudaStream_t st, int nsteps, bool use_graph, 
 // species set-up
 // ---------------------------------------------------------------------------
 
-// Slot layout: need[t] = roundup4(np[t] + extra[t]); free capacity spread in
-// proportion to need + min_slack (multiples of 4).
-static void slot_layout( const std::vector<int> & np, uint64_t max_part, int min_slack,
+// Slot layout: need[t] = roundup4(np[t]); the free capacity spread over the
+// slots in proportion to need + min_slack (multiples of 4), but for a share
+// pool_frac left after the last slot as the pool that tiles outgrowing their
+// slots move into (the sort's relocation).
+static void slot_layout( const std::vector<int> & np, uint64_t max_part, int min_slack, double pool_frac,
                          std::vector<int> & off, std::vector<int> & cap ) {
     const int nt = (int) np.size();
     off.assign( nt, 0 ); cap.assign( nt, 0 );
     long long need_sum = 0, w_sum = 0;
     for ( int t = 0; t < nt; t++ ) { const int nd = roundup4( np[t] ); need_sum += nd; w_sum += nd + min_slack; }
-    const long long free_cap = std::max<long long>( 0, (long long) max_part - need_sum );
+    const long long free_cap = (long long) ( std::max<long long>( 0, (long long) max_part - need_sum ) * ( 1.0 - pool_frac ) );
     long long o = 0;
     for ( int t = 0; t < nt; t++ ) {
         const int nd = roundup4( np[t] );
@@ -777,7 +782,7 @@ static int species_upload( zpic_sim * s, HSpecies * sp, const std::vector<int> &
     for ( int t = 0; t < nt; t++ ) { poff[t] = (int) total; total += np[t]; }
     std::vector<int> off, cap;
     const int min_slack = std::max<int>( 16, (int) ( sp->ppc[0] * sp->ppc[1] * s->nxx * s->nxy / 8 ) );
-    slot_layout( np, sp->max_part, min_slack, off, cap );
+    slot_layout( np, sp->max_part, min_slack, sp->d.pool_frac, off, cap );
     if ( (long long) off.back() + cap.back() > (long long) sp->max_part || [&] {
              for ( int t = 0; t < nt; t++ ) if ( cap[t] < np[t] ) return true; return false; }() )
         return fail( ZPIC_E_NOMEM, "particle set does not fit the species buffer" );
@@ -785,6 +790,8 @@ static int species_upload( zpic_sim * s, HSpecies * sp, const std::vector<int> &
     CK( cudaMemcpyAsync( sp->d.np, np.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
     CK( cudaMemcpyAsync( sp->d.off, off.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
     CK( cudaMemcpyAsync( sp->d.cap, cap.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
+    sp->pool_h = off.back() + cap.back();
+    CK( cudaMemcpyAsync( sp->d.pool, &sp->pool_h, sizeof( int ), cudaMemcpyHostToDevice, st ) );
     int * poff_d = nullptr;
     TRY( dalloc( &poff_d, nt ) );
     CK( cudaMemcpyAsync( poff_d, poff.data(), nt * sizeof( int ), cudaMemcpyHostToDevice, st ) );
@@ -880,15 +887,18 @@ static int species_alloc( zpic_sim * s, HSpecies * sp, uint64_t max_part ) {
     TRY( dalloc( &d.idx, max_part ) ); TRY( dalloc( &d.aux, max_part ) ); TRY( dalloc( &d.aux2, max_part ) );
     TRY( dalloc( &d.in_cnt, nt ) ); TRY( dalloc( &d.stage_cnt, nt ) );
     TRY( dalloc( &d.cnt, 9 * (size_t) nt ) ); TRY( dalloc( &d.base, 9 * (size_t) nt ) );
-    TRY( dalloc( &d.hs, nt ) ); TRY( dalloc( &d.pk, nt ) ); TRY( dalloc( &d.overflow, 1 ) );
+    TRY( dalloc( &d.hs, nt ) ); TRY( dalloc( &d.overflow, 1 ) );
+    TRY( dalloc( &d.reloc, nt ) ); TRY( dalloc( &d.pool, 1 ) );
+    CK( cudaMemset( d.reloc, 0, nt * sizeof( int ) ) );
+    CK( cudaMemset( d.pool, 0, sizeof( int ) ) );
     CK( cudaMemset( d.cnt, 0, 9 * (size_t) nt * sizeof( int ) ) );
     CK( cudaMemset( d.overflow, 0, sizeof( int ) ) );
     TRY( dalloc( &d.new_off, nt ) ); TRY( dalloc( &d.new_cap, nt ) ); TRY( dalloc( &d.new_np, nt ) );
     TRY( dalloc( &d.extra, nt ) ); TRY( dalloc( &d.mode, 1 ) );
     TRY( dalloc( &sp->inj_dyn, 4 ) ); TRY( dalloc( &sp->mw_nmove_d, 1 ) );
     CK( cudaMemset( sp->mw_nmove_d, 0, sizeof( unsigned ) ) );
-    TRY( dalloc( &d.nmove, 2 ) );
-    CK( cudaMemset( d.nmove, 0, 2 * sizeof( unsigned long long ) ) );
+    TRY( dalloc( &d.nmove, 3 ) );
+    CK( cudaMemset( d.nmove, 0, 3 * sizeof( unsigned long long ) ) );
     CK( cudaMemset( d.extra, 0, nt * sizeof( int ) ) );
     CK( cudaMemset( d.mode, 0, sizeof( int ) ) );
     return ZPIC_OK;
@@ -985,6 +995,8 @@ static void species_params( zpic_sim * s, HSpecies * sp ) {
     d.pery = sp->bc[2] == ZPIC_SPECIES_BC_PERIODIC;
     for ( int k = 0; k < 4; k++ ) d.bc[k] = sp->bc[k];
     d.min_slack = std::max<int>( 16, (int) ( sp->ppc[0] * sp->ppc[1] * s->nxx * s->nxy / 8 ) );
+    d.pool_frac = (float) s->pool_frac;
+    d.reloc_room = (float) s->reloc_room;
     d.run = 0;
 }
 
@@ -1383,6 +1395,16 @@ int zpic_b200_sim_set_option( zpic_sim * s, const char * key, double v ) {
         if ( !( v > 0 && v <= 64 ) ) return fail( ZPIC_E_INVALID, "capacity_factor must be in (0, 64]" );
         s->capacity_factor = v;
     }
+    else if ( k == "pool_fraction" || k == "relocation_room" ) {
+        // tile-slot policy: the share of the free capacity kept as a pool at
+        // the end of the buffer (tiles that outgrow their slots move there),
+        // and the room a moved tile gets, as a share of its count
+        if ( !( v >= 0 && v <= ( k == "pool_fraction" ? 0.95 : 16.0 ) ) ) return fail( ZPIC_E_INVALID, k + " out of range" );
+        if ( k == "pool_fraction" ) s->pool_frac = v; else s->reloc_room = v;
+        for ( auto * h : s->species ) species_params( s, h );
+        s->plan.release();
+        s->layout_gen++;
+    }
     else if ( k == "wait_limit" ) {
         // polls of the kernels' bounded waits on their bulk copies before
         // they give up (default ~0.5 s worth)
@@ -1754,6 +1776,16 @@ int zpic_b200_species_repacks( zpic_sim * s, int32_t sp, uint64_t * repacks ) {
     CK( cudaMemcpyAsync( &v, s->species[sp]->d.nmove + 1, sizeof( v ), cudaMemcpyDeviceToHost, s->stream ) );
     CK( cudaStreamSynchronize( s->stream ) );
     *repacks = v;
+    return ZPIC_OK;
+}
+
+int zpic_b200_species_relocations( zpic_sim * s, int32_t sp, uint64_t * tiles ) {
+    TRY( sim_select( s ) ); TRY( species_index( s, sp ) );
+    if ( !tiles ) return fail( ZPIC_E_INVALID, "null argument" );
+    unsigned long long v = 0;
+    CK( cudaMemcpyAsync( &v, s->species[sp]->d.nmove + 2, sizeof( v ), cudaMemcpyDeviceToHost, s->stream ) );
+    CK( cudaStreamSynchronize( s->stream ) );
+    *tiles = v;
     return ZPIC_OK;
 }
 

@@ -717,7 +717,18 @@ k_sort_check( const Item * __restrict__ items, int nitems, const SpDev * __restr
     const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
     S.in_cnt[t] = in;
     S.new_np[t] = stay + in;
-    if ( stay + in + ex > S.cap[t] ) atomicOr( S.overflow, 1 );
+    int rel = 0;
+    if ( stay + in + ex > S.cap[t] ) {
+        // a new slot in the pool, with room to grow (reloc_room times its
+        // count, at least twice the minimum slack): a tile that outgrew its
+        // slot is usually still growing
+        rel = 1;
+        atomicAdd( S.nmove + 2, 1ull );
+        const int grow = max( 2 * S.min_slack, (int) ( S.reloc_room * ( stay + in ) ) );
+        S.new_cap[t] = ( ( stay + in + ex + 3 ) & ~3 ) + ( ( grow + 3 ) & ~3 );
+        atomicOr( S.overflow, 1 );
+    }
+    S.reloc[t] = rel;
 }
 
 constexpr int PLAN_THREADS = 1024;
@@ -745,6 +756,25 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
     const int per = ( nt + PLAN_THREADS - 1 ) / PLAN_THREADS;
     const int t0 = min( nt, (int) threadIdx.x * per ), t1 = min( nt, t0 + per );
     __shared__ long long s_total;
+    // relocation (mode 3): the tiles that outgrew their slots get new slots
+    // from the pool, everything else sorts in place; a repack only when the
+    // pool cannot hold them
+    {
+        long long rsum = 0;
+        for ( int t = t0; t < t1; t++ ) if ( S.reloc[t] ) rsum += S.new_cap[t];
+        long long ro = block_exscan< PLAN_THREADS >( rsum, &s_total );
+        const long long rtotal = s_total;
+        const long long pool = *S.pool;
+        if ( pool + rtotal <= (long long) S.max_part ) {
+            ro += pool;
+            for ( int t = t0; t < t1; t++ )
+                if ( S.reloc[t] ) { S.new_off[t] = (int) ro; ro += S.new_cap[t]; }
+            __syncthreads();                      // every thread has read the pool start
+            if ( threadIdx.x == 0 ) { *S.pool = (int) ( pool + rtotal ); *S.mode = 3; }
+            return;
+        }
+        __syncthreads();
+    }
     long long need_sum = 0, w_sum = 0, np_sum = 0;
     for ( int t = t0; t < t1; t++ ) {
         const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
@@ -768,23 +798,22 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
         if ( threadIdx.x == 0 ) { *S.mode = 2; atomicOr( R.status, ST_CAPACITY ); }
         return;
     }
-    long long cap_sum = 0, nnp_sum = 0;
+    // the free capacity: slack in the slots, a share (pool_frac) left as the pool
+    const long long spread = (long long) ( (double) free_cap * ( 1.0 - S.pool_frac ) );
+    long long cap_sum = 0;
     for ( int t = t0; t < t1; t++ ) {
         const int ex = ( use_extra && S.extra ) ? S.extra[t] : 0;
         const int need = ( S.new_np[t] + ex + 3 ) & ~3;
-        const long long slack = w_total > 0 ? ( free_cap * ( need + S.min_slack ) ) / w_total : 0;
+        const long long slack = w_total > 0 ? ( spread * ( need + S.min_slack ) ) / w_total : 0;
         const int c = need + (int) ( slack & ~3LL );
         S.new_cap[t] = c;
         cap_sum += c;
-        nnp_sum += S.new_np[t];
     }
     __syncthreads();
     long long pc = block_exscan< PLAN_THREADS >( cap_sum, &s_total );
     for ( int t = t0; t < t1; t++ ) { S.new_off[t] = (int) pc; pc += S.new_cap[t]; }
-    __syncthreads();
-    long long pn = block_exscan< PLAN_THREADS >( nnp_sum, &s_total );
-    for ( int t = t0; t < t1; t++ ) { S.pk[t] = (int) pn; pn += S.new_np[t]; }
     if ( threadIdx.x == 0 ) {
+        *S.pool = (int) s_total;
         *S.mode = 1;
         S.nmove[1] += 1;
         rlist[ 1 + atomicAdd( rlist, 1 ) ] = species_list[ blockIdx.x ];
@@ -848,22 +877,24 @@ __device__ __noinline__ void repack_out( const SpDev & S, const RunDev & R ) {
     }
 }
 
-// Repack, second half: B -> A, the particles of the new layout only (its
-// slack is not copied), by packed index over the new counts (pk, the plan's
-// prefix of new_np), so consecutive threads copy consecutive slots.
+// Repack, second half: B -> A over the whole buffer (slack included),
+// 16-byte vectors (the arrays are cudaMalloc'd, 256-byte aligned); the last
+// max_part % 4 entries are copied singly.  A sweep of the whole buffer in
+// vectors is faster than visiting only the new layout's particles, which
+// needs a search for each one's tile.
+__device__ __forceinline__ void copy_vec( void * dst, const void * src, long long i ) {
+    reinterpret_cast<uint4 *>( dst )[i] = reinterpret_cast<const uint4 *>( src )[i];
+}
+
 __device__ __noinline__ void repack_in( const SpDev & S ) {
-    const int nt = S.ntiles;
-    const long long n = (long long) S.pk[ nt - 1 ] + S.new_np[ nt - 1 ];
+    const long long n = S.max_part, n4 = n / 4;
     const long long stride = (long long) gridDim.x * blockDim.x;
-    for ( long long q = (long long) blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride ) {
-        int lo = 0, hi = nt - 1;
-        while ( lo < hi ) {
-            const int mid = ( lo + hi + 1 ) >> 1;
-            if ( S.pk[mid] <= q ) lo = mid; else hi = mid - 1;
-        }
-        const size_t p = (size_t) S.new_off[lo] + ( q - S.pk[lo] );
-        copy_particle( S.A, p, S.B, p );
+    for ( long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride ) {
+        copy_vec( S.A.cell, S.B.cell, i ); copy_vec( S.A.xx, S.B.xx, i ); copy_vec( S.A.xy, S.B.xy, i );
+        copy_vec( S.A.ux, S.B.ux, i );     copy_vec( S.A.uy, S.B.uy, i ); copy_vec( S.A.uz, S.B.uz, i );
     }
+    for ( long long p = 4 * n4 + blockIdx.x * (long long) blockDim.x + threadIdx.x; p < n; p += stride )
+        copy_particle( S.A, (size_t) p, S.B, (size_t) p );
 }
 
 // Per tile (WPT warps per tile; 1 when there are many tiles, a whole CTA when
@@ -889,14 +920,16 @@ k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restr
     if ( WPT > 1 ) __syncthreads(); else __syncwarp();
 
     const int wi = blockIdx.x * TPB + tib;
-    bool active = wi < nitems;
+    bool active = wi < nitems, rel = false;
     Item it{};
     const SpDev * Sp = nullptr;
     if ( active ) {
         it = items[ wi ];
         Sp = &sps[ it.sp ];
         if ( sub == 0 && lane < 9 ) Sp->cnt[ 9 * it.tile + lane ] = 0;
-        active = *Sp->mode == 0;
+        const int mode = *Sp->mode;
+        active = mode == 0 || mode == 3;
+        rel = active && mode == 3 && Sp->reloc[ it.tile ];
     }
     int t = 0, np = 0, nl = 0, nn = 0, off = 0, nxx = 1, nxy = 1;
     if ( active ) {
@@ -905,6 +938,32 @@ k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restr
         t = it.tile; nxx = R.nxx; nxy = R.nxy;
         np = S.np[t]; nl = S.nidx[t]; off = S.off[t];
         nn = np - nl + S.in_cnt[t];
+    }
+    if ( rel ) {
+        // a tile that outgrew its slot: its stayers, compacted into its new
+        // slot from the pool (contiguous writes); the incoming follow them
+        const SpDev & S = *Sp;
+        const size_t noff = (size_t) S.new_off[t];
+        for ( int c0 = sub * 32 * SU; c0 < np; c0 += WPT * 32 * SU ) {
+            uint32_t c[SU];
+#pragma unroll
+            for ( int u = 0; u < SU; u++ ) {
+                const int ci = c0 + u * 32 + lane;
+                c[u] = ci < np ? S.A.cell[ (size_t) off + ci ] : 0x80008000u;
+            }
+#pragma unroll
+            for ( int u = 0; u < SU; u++ ) {
+                const int ix = cell_x( c[u] ), iy = cell_y( c[u] );
+                const bool stay = ix >= 0 && ix < nxx && iy >= 0 && iy < nxy;
+                const unsigned m = __ballot_sync( 0xffffffffu, stay );
+                int b = 0;
+                if ( lane == 0 && m ) b = atomicAdd( &s_ns[tib], __popc( m ) );
+                b = __shfl_sync( 0xffffffffu, b, 0 );
+                if ( stay ) copy_particle( S.A, noff + b + __popc( m & lt ), S.A, (size_t) off + c0 + u * 32 + lane );
+            }
+        }
+    } else if ( active ) {
+        const SpDev & S = *Sp;
         // leavers' slots below nn, SU per lane in flight
         for ( int k0 = sub * 32 * SU; k0 < nl; k0 += WPT * 32 * SU ) {
             int i[SU];
@@ -944,6 +1003,16 @@ k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restr
         }
     }
     if ( WPT > 1 ) __syncthreads(); else __syncwarp();
+    if ( rel ) {
+        // incoming particles go after the stayers (direct positions, no list)
+        const SpDev & S = *Sp;
+        const int ns = s_ns[tib];
+        if ( sub == 0 && lane == 0 ) {
+            S.hs[t] = ns;
+            if ( ns != np - nl ) { S.hs[t] = nn; atomicOr( runs[ S.run ].status, ST_BAD_CELL ); }
+        }
+        active = false;
+    }
     if ( active ) {
         const SpDev & S = *Sp;
         const int ne = s_ne[tib], ns = s_ns[tib];
@@ -1001,6 +1070,7 @@ k_sort_scatter( const Item * __restrict__ items, int nitems, const SpDev * __res
     __shared__ int s_off[TPB][9];                 // off[tt] of the target through direction d
     __shared__ int s_aux[TPB][9];                 // its list position of the first slot for d (-1: dropped)
     __shared__ int s_cap[TPB][9];                 // new count of the target (bound of its list and slots)
+    __shared__ int s_dir[TPB][9];                 // 1: relocated target, positions without the list
 
     const int wi = blockIdx.x * TPB + tib;
     bool active = wi < nitems;
@@ -1011,21 +1081,25 @@ k_sort_scatter( const Item * __restrict__ items, int nitems, const SpDev * __res
         it = items[ wi ];
         Sp = &sps[ it.sp ];
         mode = *Sp->mode;
-        active = mode == 0;
+        active = mode == 0 || mode == 3;
     }
     if ( active && sub == 0 && lane < 9 ) {
         const SpDev & S = *Sp;
         const RunDev & R = runs[ S.run ];
         const int tt = lane == 4 ? -1 : neighbor_tile( it.tile, lane, R.ntx, R.nty, S.perx, S.pery );
-        int o = 0, a = -1, nn = 0;
+        int o = 0, a = -1, nn = 0, dr = 0;
         if ( tt >= 0 ) {
-            o = S.off[tt];
+            // a relocated target takes its incoming right after its stayers in
+            // its new slot; the others through their empty-slot list
+            dr = mode == 3 && S.reloc[tt];
+            o = dr ? S.new_off[tt] : S.off[tt];
             a = S.hs[tt] + S.base[ 9 * tt + lane ];
             nn = S.new_np[tt];
         }
         s_off[tib][lane] = o;
         s_aux[tib][lane] = a;
         s_cap[tib][lane] = nn;
+        s_dir[tib][lane] = dr;
         s_rank[tib][lane] = 0;
     }
     if ( WPT > 1 ) __syncthreads(); else __syncwarp();
@@ -1068,7 +1142,7 @@ k_sort_scatter( const Item * __restrict__ items, int nitems, const SpDev * __res
                     // (anything else means inconsistent counts: reported, the
                     // particle is not written)
                     const int r = s_aux[tib][d] + b + __popc( peers & lt );
-                    slot[u] = r < s_cap[tib][d] ? S.aux[ (size_t) s_off[tib][d] + r ] : -1;
+                    slot[u] = r < s_cap[tib][d] ? ( s_dir[tib][d] ? r : S.aux[ (size_t) s_off[tib][d] + r ] ) : -1;
                 }
             }
 #pragma unroll
@@ -1090,11 +1164,11 @@ k_sort_scatter( const Item * __restrict__ items, int nitems, const SpDev * __res
     }
     // every warp of the tile has read nidx before it is cleared
     if ( WPT > 1 ) __syncthreads(); else __syncwarp();
-    if ( ( mode == 0 || mode == 1 ) && sub == 0 && lane == 0 ) {
+    if ( mode >= 0 && mode != 2 && sub == 0 && lane == 0 ) {
         const SpDev & S = *Sp;
         const int t = it.tile;
-        if ( mode == 0 ) S.np[t] = S.new_np[t];
-        else { S.np[t] = S.new_np[t]; S.off[t] = S.new_off[t]; S.cap[t] = S.new_cap[t]; }
+        S.np[t] = S.new_np[t];
+        if ( mode == 1 || ( mode == 3 && S.reloc[t] ) ) { S.off[t] = S.new_off[t]; S.cap[t] = S.new_cap[t]; }
         S.nidx[t] = 0;
     }
     const int nr = rlist[0];

@@ -67,14 +67,15 @@ struct SpDev {
     int * in_cnt;                 // [ntiles] incoming particles (sort check)
     int * hs;                     // [ntiles] stayers moved down inside the tile (sort); in a repack:
                                   // packed position of each tile's first particle, old layout
-    int * pk;                     // [ntiles] repack: packed position of each tile's first particle, new layout
     int * overflow;               // [1] a tile's new count exceeds its slot (sort check)
+    int * reloc;                  // [ntiles] 1: the tile outgrew its slot and moves to the pool (sort check)
+    int * pool;                   // [1] start of the free pool after the last slot (pool ends at max_part)
     int * stage_cnt;              // [ntiles] repack fill counters
     int * new_off; int * new_cap; int * new_np;  // [ntiles] new counts, repack layout
     int * extra;                  // [ntiles] room to reserve for injection (or nullptr)
-    int * mode;                   // [1] 0 = in-place sort, 1 = repack, 2 = no room
+    int * mode;                   // [1] 0 in-place sort, 1 repack, 2 no room, 3 in place with relocated tiles
     double * energy;              // [ntiles*nchunk] per work-item kinetic energy sums
-    unsigned long long * nmove;   // [0] pushes counter, [1] repacks of the tile slots
+    unsigned long long * nmove;   // [0] pushes counter, [1] repacks of the tile slots, [2] tiles relocated
     float alpha;                  // 0.5*dt/m_q (species.cpp:2305)
     float dt_dx, dt_dy;           // dt/dx (species.cpp:2140-2143)
     float q;                      // charge per particle
@@ -82,6 +83,8 @@ struct SpDev {
     int perx, pery;               // particle periodic flags
     int bc[4];                    // species::bc
     int min_slack;                // minimum free slots per tile after a repack
+    float pool_frac;              // share of the free capacity kept as the pool at a repack (option "pool_fraction")
+    float reloc_room;             // room given to a relocated tile, as a share of its count (option "relocation_room")
     float jscale;                 // fixed-point tile current: 2^k with |q| * jscale < 2^30
     double jscale_inv;            // 1 / jscale
 };

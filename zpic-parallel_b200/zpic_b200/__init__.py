@@ -48,7 +48,7 @@ EXPORTS = [
     'zpic_b200_species_move', 'zpic_b200_species_process_bc', 'zpic_b200_species_tile_sort',
     'zpic_b200_species_set_bc', 'zpic_b200_species_set_push_type', 'zpic_b200_species_energy',
     'zpic_b200_species_nmove', 'zpic_b200_species_np_total', 'zpic_b200_species_np_max_tile',
-    'zpic_b200_species_max_part',
+    'zpic_b200_species_max_part', 'zpic_b200_species_relocations',
     'zpic_b200_species_get_tiles', 'zpic_b200_species_get', 'zpic_b200_species_set',
     'zpic_b200_species_gather', 'zpic_b200_species_charge', 'zpic_b200_species_phasespace',
     'zpic_b200_grid_size', 'zpic_b200_grid_get', 'zpic_b200_grid_set', 'zpic_b200_grid_gather',
@@ -121,6 +121,7 @@ def lib():
             'zpic_b200_batch_launch_count': (I, [P, ctypes.POINTER(ctypes.c_uint64)]),
             'zpic_b200_sim_autotune': (I, [P, I, IP]),
             'zpic_b200_species_repacks': (I, [P, I, U64P]),
+            'zpic_b200_species_relocations': (I, [P, I, U64P]),
             'zpic_b200_batch_autotune': (I, [P, I, IP]),
             'zpic_b200_emf_set_bc': (I, [P, IP]),
             'zpic_b200_emf_advance': (I, [P, I]),
@@ -353,6 +354,12 @@ class Simulation:
         """Times the tile sort rebuilt the slot layout of species sp."""
         v = ctypes.c_uint64()
         _check(lib().zpic_b200_species_repacks(self.h, sp, ctypes.byref(v)))
+        return v.value
+
+    def relocations(self, sp):
+        """Tiles of species sp that outgrew their slot and moved into the pool."""
+        v = ctypes.c_uint64()
+        _check(lib().zpic_b200_species_relocations(self.h, sp, ctypes.byref(v)))
         return v.value
 
     def np_total(self, sp):
