@@ -167,9 +167,20 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  *                         their initial level; 0 never (default).  Order only:
  *                         every tile keeps its particle multiset.
  *   "capacity_factor" f   initial particle capacity of species added after
- *                         this call: f * cells * ppc (default 1.2, the
- *                         reference's max_part, species.cpp:1752); buffers grow
- *                         when injection or species_set needs more
+ *                         this call: f * cells * ppc (default 1.6; the
+ *                         reference's max_part is 1.2 * cells * ppc,
+ *                         species.cpp:1752, for a layout without per-tile
+ *                         room); buffers grow when injection or species_set
+ *                         needs more
+ *   "pool_fraction"  f    share of the free particle capacity kept as a pool
+ *                         after the last tile slot (default 0.25); a tile whose
+ *                         particles outgrow its slot moves into the pool, and
+ *                         only when the pool is short is the whole layout
+ *                         rebuilt.  Set before adding species to affect their
+ *                         first layout.  Order only: results do not change
+ *   "relocation_room" r   room a moved tile gets beyond its particles, as a
+ *                         share of their number (default 0.5; at least twice
+ *                         the minimum slack of ppc * cells / 8)
  *   "wait_limit"     n    polls before a kernel's bounded wait on its bulk
  *                         copies gives up (default 4194304, ~0.5 s); a kernel
  *                         that gives up skips its work for that tile and the

@@ -143,6 +143,7 @@ struct HSpecies {
         dfree( d.np ); dfree( d.off ); dfree( d.cap ); dfree( d.nidx ); dfree( d.idx );
         dfree( d.aux ); dfree( d.aux2 ); dfree( d.in_cnt ); dfree( d.stage_cnt );
         dfree( d.cnt ); dfree( d.base ); dfree( d.hs ); dfree( d.overflow ); dfree( d.reloc ); dfree( d.pool );
+        dfree( d.rel_tile ); dfree( d.rel_start ); dfree( d.rel_n );
         dfree( d.new_off ); dfree( d.new_cap ); dfree( d.new_np ); dfree( d.extra ); dfree( d.mode );
         dfree( d.energy ); dfree( d.nmove ); dfree( inj_dyn ); dfree( mw_nmove_d );
     }
@@ -251,10 +252,14 @@ struct zpic_sim {
     int reorder_every = REORDER_DEFAULT;
     int chunks_opt = 0;
     int jacc = 2;                   // fixed-point tile current (option "jacc")
-    double pool_frac = 0.5;         // share of free particle capacity kept as the pool (option "pool_fraction")
-    double reloc_room = 1.0;        // room for a relocated tile, share of its count (option "relocation_room")
-    double capacity_factor = 1.2;   // initial particle capacity per cell and ppc (option "capacity_factor";
-                                    // the reference's max_part = 1.2 cells ppc, species.cpp:1752)
+    double pool_frac = 0.25;        // share of free particle capacity kept as the pool (option "pool_fraction")
+    double reloc_room = 0.5;        // room for a relocated tile, share of its count (option "relocation_room")
+    // Initial particle capacity per cell and ppc (option "capacity_factor").
+    // The reference's max_part = 1.2 cells ppc (species.cpp:1752) serves a
+    // packed layout that is rebuilt every step; tile slots need room per
+    // tile, and with 1.2 a filamenting Weibel plasma rebuilt its slots every
+    // ~15 steps (9.0 k vs 9.3 k run-steps/s on the 256-run ensemble at 1.6).
+    double capacity_factor = 1.6;
     int profile = 0;                // 1: per-phase events, steps issued eagerly; 2: the same inside CUDA graphs
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[PH_N];
     double phase_ms[PH_N] = { 0 };
@@ -889,6 +894,8 @@ static int species_alloc( zpic_sim * s, HSpecies * sp, uint64_t max_part ) {
     TRY( dalloc( &d.cnt, 9 * (size_t) nt ) ); TRY( dalloc( &d.base, 9 * (size_t) nt ) );
     TRY( dalloc( &d.hs, nt ) ); TRY( dalloc( &d.overflow, 1 ) );
     TRY( dalloc( &d.reloc, nt ) ); TRY( dalloc( &d.pool, 1 ) );
+    TRY( dalloc( &d.rel_tile, nt ) ); TRY( dalloc( &d.rel_start, nt + 1 ) ); TRY( dalloc( &d.rel_n, 1 ) );
+    CK( cudaMemset( d.rel_n, 0, sizeof( int ) ) );
     CK( cudaMemset( d.reloc, 0, nt * sizeof( int ) ) );
     CK( cudaMemset( d.pool, 0, sizeof( int ) ) );
     CK( cudaMemset( d.cnt, 0, 9 * (size_t) nt * sizeof( int ) ) );

@@ -732,6 +732,9 @@ k_sort_check( const Item * __restrict__ items, int nitems, const SpDev * __restr
 }
 
 constexpr int PLAN_THREADS = 1024;
+// rlist entries: species index, with this bit set for a species that only
+// relocates tiles (mode 3) rather than repacking (mode 1)
+constexpr int RLIST_RELOCATE = 1 << 30;
 
 // One CTA per species.  In place (mode 0) unless a tile overflowed its slot;
 // then the repack layout (mode 1): need[t] = new count + injection reserve,
@@ -760,17 +763,33 @@ k_sort_plan( const SpDev * __restrict__ sps, const int * __restrict__ species_li
     // from the pool, everything else sorts in place; a repack only when the
     // pool cannot hold them
     {
-        long long rsum = 0;
-        for ( int t = t0; t < t1; t++ ) if ( S.reloc[t] ) rsum += S.new_cap[t];
+        long long rsum = 0, rn = 0, rp = 0;
+        for ( int t = t0; t < t1; t++ )
+            if ( S.reloc[t] ) { rsum += S.new_cap[t]; rn += 1; rp += S.np[t]; }
         long long ro = block_exscan< PLAN_THREADS >( rsum, &s_total );
         const long long rtotal = s_total;
         const long long pool = *S.pool;
         if ( pool + rtotal <= (long long) S.max_part ) {
+            // new slots, and the list of the relocated tiles with the packed
+            // start of their particles (the local kernel's grid-stride copy)
+            long long ri = block_exscan< PLAN_THREADS >( rn, &s_total );
+            const long long nrel = s_total;
+            long long rs = block_exscan< PLAN_THREADS >( rp, &s_total );
+            const long long ptotal = s_total;
             ro += pool;
             for ( int t = t0; t < t1; t++ )
-                if ( S.reloc[t] ) { S.new_off[t] = (int) ro; ro += S.new_cap[t]; }
+                if ( S.reloc[t] ) {
+                    S.new_off[t] = (int) ro; ro += S.new_cap[t];
+                    S.rel_tile[ri] = t; S.rel_start[ri] = (int) rs; ri += 1; rs += S.np[t];
+                    S.hs[t] = S.np[t] - S.nidx[t];  // the stayers, then the incoming
+                    S.stage_cnt[t] = 0;
+                }
             __syncthreads();                      // every thread has read the pool start
-            if ( threadIdx.x == 0 ) { *S.pool = (int) ( pool + rtotal ); *S.mode = 3; }
+            if ( threadIdx.x == 0 ) {
+                *S.pool = (int) ( pool + rtotal ); *S.mode = 3;
+                S.rel_start[ nrel ] = (int) ptotal; *S.rel_n = (int) nrel;
+                rlist[ 1 + atomicAdd( rlist, 1 ) ] = species_list[ blockIdx.x ] | RLIST_RELOCATE;
+            }
             return;
         }
         __syncthreads();
@@ -877,6 +896,42 @@ __device__ __noinline__ void repack_out( const SpDev & S, const RunDev & R ) {
     }
 }
 
+// Relocation (mode 3): the stayers of every tile that outgrew its slot are
+// copied into its new slot from the pool.  The whole grid strides over those
+// tiles' particles in packed order (rel_start, written by the plan), so a big
+// tile is spread over all CTAs; places in the new slot are claimed per tile
+// with one atomic per group of lanes in the same tile.
+__device__ __noinline__ void relocate_out( const SpDev & S, const RunDev & R ) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = ( 1u << lane ) - 1u;
+    const int nrel = *S.rel_n, nxx = R.nxx, nxy = R.nxy;
+    if ( nrel <= 0 ) return;
+    const long long n = S.rel_start[ nrel ];
+    for ( long long q0 = (long long) blockIdx.x * blockDim.x; q0 < n; q0 += (long long) gridDim.x * blockDim.x ) {
+        const long long q = q0 + threadIdx.x;
+        int t = -1;
+        long long p = 0;
+        if ( q < n ) {
+            int lo = 0, hi = nrel - 1;
+            while ( lo < hi ) {
+                const int mid = ( lo + hi + 1 ) >> 1;
+                if ( S.rel_start[mid] <= q ) lo = mid; else hi = mid - 1;
+            }
+            const int tt = S.rel_tile[lo];
+            p = (long long) S.off[tt] + ( q - S.rel_start[lo] );
+            const uint32_t c = S.A.cell[p];
+            const int ix = cell_x( c ), iy = cell_y( c );
+            if ( ix >= 0 && ix < nxx && iy >= 0 && iy < nxy ) t = tt;    // leavers are in the outbox
+        }
+        const unsigned same = __match_any_sync( 0xffffffffu, t );
+        const int leader = __ffs( same ) - 1;
+        int base = 0;
+        if ( t >= 0 && lane == leader ) base = atomicAdd( S.stage_cnt + t, __popc( same ) );
+        base = __shfl_sync( same, base, leader );
+        if ( t >= 0 ) copy_particle( S.A, (size_t) S.new_off[t] + base + __popc( same & lt ), S.A, (size_t) p );
+    }
+}
+
 // Repack, second half: B -> A over the whole buffer (slack included),
 // 16-byte vectors (the arrays are cudaMalloc'd, 256-byte aligned); the last
 // max_part % 4 entries are copied singly.  A sweep of the whole buffer in
@@ -939,30 +994,7 @@ k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restr
         np = S.np[t]; nl = S.nidx[t]; off = S.off[t];
         nn = np - nl + S.in_cnt[t];
     }
-    if ( rel ) {
-        // a tile that outgrew its slot: its stayers, compacted into its new
-        // slot from the pool (contiguous writes); the incoming follow them
-        const SpDev & S = *Sp;
-        const size_t noff = (size_t) S.new_off[t];
-        for ( int c0 = sub * 32 * SU; c0 < np; c0 += WPT * 32 * SU ) {
-            uint32_t c[SU];
-#pragma unroll
-            for ( int u = 0; u < SU; u++ ) {
-                const int ci = c0 + u * 32 + lane;
-                c[u] = ci < np ? S.A.cell[ (size_t) off + ci ] : 0x80008000u;
-            }
-#pragma unroll
-            for ( int u = 0; u < SU; u++ ) {
-                const int ix = cell_x( c[u] ), iy = cell_y( c[u] );
-                const bool stay = ix >= 0 && ix < nxx && iy >= 0 && iy < nxy;
-                const unsigned m = __ballot_sync( 0xffffffffu, stay );
-                int b = 0;
-                if ( lane == 0 && m ) b = atomicAdd( &s_ns[tib], __popc( m ) );
-                b = __shfl_sync( 0xffffffffu, b, 0 );
-                if ( stay ) copy_particle( S.A, noff + b + __popc( m & lt ), S.A, (size_t) off + c0 + u * 32 + lane );
-            }
-        }
-    } else if ( active ) {
+    if ( active && !rel ) {
         const SpDev & S = *Sp;
         // leavers' slots below nn, SU per lane in flight
         for ( int k0 = sub * 32 * SU; k0 < nl; k0 += WPT * 32 * SU ) {
@@ -1003,16 +1035,9 @@ k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restr
         }
     }
     if ( WPT > 1 ) __syncthreads(); else __syncwarp();
-    if ( rel ) {
-        // incoming particles go after the stayers (direct positions, no list)
-        const SpDev & S = *Sp;
-        const int ns = s_ns[tib];
-        if ( sub == 0 && lane == 0 ) {
-            S.hs[t] = ns;
-            if ( ns != np - nl ) { S.hs[t] = nn; atomicOr( runs[ S.run ].status, ST_BAD_CELL ); }
-        }
-        active = false;
-    }
+    // a tile that outgrew its slot: its stayers are copied by the whole grid
+    // below (relocate_out); the incoming follow them in the new slot
+    if ( rel ) active = false;
     if ( active ) {
         const SpDev & S = *Sp;
         const int ne = s_ne[tib], ns = s_ns[tib];
@@ -1046,8 +1071,10 @@ k_sort_local( const Item * __restrict__ items, int nitems, const SpDev * __restr
     }
     const int nr = rlist[0];
     for ( int k = 0; k < nr; k++ ) {
-        const SpDev & S = sps[ rlist[ 1 + k ] ];
-        repack_out( S, runs[ S.run ] );
+        const int e = rlist[ 1 + k ];
+        const SpDev & S = sps[ e & ~RLIST_RELOCATE ];
+        if ( e & RLIST_RELOCATE ) relocate_out( S, runs[ S.run ] );
+        else repack_out( S, runs[ S.run ] );
     }
 }
 
@@ -1172,7 +1199,8 @@ k_sort_scatter( const Item * __restrict__ items, int nitems, const SpDev * __res
         S.nidx[t] = 0;
     }
     const int nr = rlist[0];
-    for ( int k = 0; k < nr; k++ ) repack_in( sps[ rlist[ 1 + k ] ] );
+    for ( int k = 0; k < nr; k++ )
+        if ( !( rlist[ 1 + k ] & RLIST_RELOCATE ) ) repack_in( sps[ rlist[ 1 + k ] ] );
 }
 
 // ---------------------------------------------------------------------------
@@ -1490,8 +1518,8 @@ __global__ void k_np_stats( const SpDev * __restrict__ sps, int sp, unsigned lon
 // so round r lists one particle of every cell that holds more than r, in
 // ascending cell order, and consecutive lanes again see consecutive cells.
 // The rank comes from a shared-memory counter per cell (its order between
-// particles of one cell is arbitrary; the ranks are kept in the leaver index
-// list, free between steps); the position of (r, c) is the number of
+// particles of one cell is arbitrary; the ranks stay in shared memory, beside
+// the tile's cells, which are read once); the position of (r, c) is the number of
 // particles in the rounds before r plus the cells before c in round r,
 // counted with a bit mask of the cells present in each round.  The tile is
 // then permuted in place one particle array at a time through shared memory
@@ -1515,26 +1543,34 @@ k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, cons
     const size_t off = S.off[t];
     const int nxx = R.nxx, nxy = R.nxy, ncell = nxx * nxy;
     const int ncw = ( ncell + 31 ) >> 5;
-    // shared memory: [buf: np_max words][inv: np_max 16-bit][cnt: ncw*32][base: max_rounds+1]
-    //                [flags: 4][masks: max_rounds*ncw words][word prefix: max_rounds*ncw 16-bit]
+    // shared memory: [buf: np_max words][inv: np_max 16-bit][rank: np_max 16-bit][cnt: ncw*32]
+    //                [base: max_rounds+1][flags: 4][masks: max_rounds*ncw words][word prefix: max_rounds*ncw 16-bit]
     uint32_t * buf = reinterpret_cast<uint32_t *>( smem_raw );
     uint16_t * inv = reinterpret_cast<uint16_t *>( buf + np_max );
-    int * cnt = reinterpret_cast<int *>( inv + np_max );
+    uint16_t * rank = inv + np_max;
+    int * cnt = reinterpret_cast<int *>( rank + np_max );
     int * base = cnt + ncw * 32;
     int * flags = base + max_rounds + 1;
     uint32_t * masks = reinterpret_cast<uint32_t *>( flags + 4 );
     uint16_t * wpre = reinterpret_cast<uint16_t *>( masks + max_rounds * ncw );
-    int * rank = S.idx + off;
+    const int n4 = np >> 2;
 
+    // the tile's cells, read once into shared memory
+    {
+        const uint32_t * g = S.A.cell + off;
+        for ( int v = threadIdx.x; v < n4; v += blockDim.x )
+            reinterpret_cast<uint4 *>( buf )[v] = reinterpret_cast<const uint4 *>( g )[v];
+        for ( int p = 4 * n4 + threadIdx.x; p < np; p += blockDim.x ) buf[p] = g[p];
+    }
     for ( int c = threadIdx.x; c < ncw * 32; c += blockDim.x ) cnt[c] = 0;
     if ( threadIdx.x == 0 ) { flags[0] = 0; flags[1] = 0; }
     __syncthreads();
     for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
-        const uint32_t cl = S.A.cell[ off + i ];
+        const uint32_t cl = buf[i];
         const int ix = cell_x( cl ), iy = cell_y( cl );
         if ( ix < 0 || ix >= nxx || iy < 0 || iy >= nxy ) { flags[0] = 1; continue; }
         const int r = atomicAdd( cnt + ix + nxx * iy, 1 );
-        rank[i] = r;
+        rank[i] = (uint16_t) r;
         if ( r >= max_rounds ) flags[0] = 1;
         else atomicMax( flags + 1, r + 1 );
     }
@@ -1576,7 +1612,7 @@ k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, cons
     }
     __syncthreads();
     for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
-        const uint32_t cl = S.A.cell[ off + i ];
+        const uint32_t cl = buf[i];
         const int c = cell_x( cl ) + nxx * cell_y( cl );
         const int r = rank[i];
         const int w = c >> 5;
@@ -1587,14 +1623,15 @@ k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, cons
     uint32_t * arr[6] = { S.A.cell, reinterpret_cast<uint32_t *>( S.A.xx ), reinterpret_cast<uint32_t *>( S.A.xy ),
                           reinterpret_cast<uint32_t *>( S.A.ux ), reinterpret_cast<uint32_t *>( S.A.uy ),
                           reinterpret_cast<uint32_t *>( S.A.uz ) };
-    const int n4 = np >> 2;
     for ( int a = 0; a < 6; a++ ) {
         uint32_t * g = arr[a] + off;
         __syncthreads();
-        for ( int v = threadIdx.x; v < n4; v += blockDim.x )
-            reinterpret_cast<uint4 *>( buf )[v] = reinterpret_cast<const uint4 *>( g )[v];
-        for ( int p = 4 * n4 + threadIdx.x; p < np; p += blockDim.x ) buf[p] = g[p];
-        __syncthreads();
+        if ( a > 0 ) {                            // the cells are in buf already
+            for ( int v = threadIdx.x; v < n4; v += blockDim.x )
+                reinterpret_cast<uint4 *>( buf )[v] = reinterpret_cast<const uint4 *>( g )[v];
+            for ( int p = 4 * n4 + threadIdx.x; p < np; p += blockDim.x ) buf[p] = g[p];
+            __syncthreads();
+        }
         for ( int v = threadIdx.x; v < n4; v += blockDim.x ) {
             const int p = 4 * v;
             reinterpret_cast<uint4 *>( g )[v] = make_uint4( buf[ inv[p] ], buf[ inv[p + 1] ], buf[ inv[p + 2] ], buf[ inv[p + 3] ] );
@@ -1755,9 +1792,11 @@ cudaError_t launch_reorder( cudaStream_t st, const Item * items, int nitems, con
     const int rounds = std::max( 1, std::min( 511, ( 32 * 1024 ) / ( 6 * ncw ) - 1 ) );
     const size_t fixed = (size_t) ncw * 32 * 4 + ( rounds + 1 ) * 4 + 16 + (size_t) rounds * ncw * 6;
     const size_t budget = 227 * 1024;
-    if ( fixed + 64 * 6 > budget ) return cudaSuccess;
-    const int np_max = std::min<size_t>( 65532, ( ( budget - fixed ) / 6 ) & ~(size_t) 7 );
-    const size_t smem = (size_t) np_max * 6 + fixed;
+    if ( fixed + 64 * 8 > budget ) return cudaSuccess;
+    // per particle: one 4-byte word of the array being permuted, a 16-bit
+    // source index and a 16-bit rank
+    const int np_max = std::min<size_t>( 65532, ( ( budget - fixed ) / 8 ) & ~(size_t) 7 );
+    const size_t smem = (size_t) np_max * 8 + fixed;
     cudaFuncSetAttribute( (const void *) k_reorder, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
     k_reorder<<< nitems, RO_THREADS, smem, st >>>( items, sps, runs, rounds, np_max );
     return cudaGetLastError();

@@ -70,6 +70,9 @@ struct SpDev {
     int * overflow;               // [1] a tile's new count exceeds its slot (sort check)
     int * reloc;                  // [ntiles] 1: the tile outgrew its slot and moves to the pool (sort check)
     int * pool;                   // [1] start of the free pool after the last slot (pool ends at max_part)
+    int * rel_tile;               // [ntiles] relocated tiles of the current sort, in tile order (plan)
+    int * rel_start;              // [ntiles + 1] their particles' packed starts; [nrel] = total (plan)
+    int * rel_n;                  // [1] number of relocated tiles (plan)
     int * stage_cnt;              // [ntiles] repack fill counters
     int * new_off; int * new_cap; int * new_np;  // [ntiles] new counts, repack layout
     int * extra;                  // [ntiles] room to reserve for injection (or nullptr)
