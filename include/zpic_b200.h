@@ -164,7 +164,8 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  *                         cell round-robin order (one particle of every cell,
  *                         cells ascending, then the next round), which keeps
  *                         the particle kernel's shared-memory bank conflicts at
- *                         their initial level; 0 never (default).  Order only:
+ *                         their initial level; 0 never.  Default: every 50
+ *                         steps, never in a moving-window run.  Order only:
  *                         every tile keeps its particle multiset.
  *   "capacity_factor" f   initial particle capacity of species added after
  *                         this call: f * cells * ppc (default 1.6; the
