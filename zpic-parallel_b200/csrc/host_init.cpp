@@ -347,13 +347,19 @@ void kernel3_x( HGrid & h, float a, float b, float c ) {
     copy_to_gc( h, 1 );
 }
 
-// laser.cpp:20-70
-void div_corr_x( HGrid & E, HGrid & B, const float dx[2] ) {
+// laser.cpp:20-70; tile rows are independent (the sums run along x), so
+// they are spread over host threads when there are enough of them
+struct DivCorrCtx { HGrid * E; HGrid * B; double dx_dy; };
+
+void div_corr_rows( int ty0, int ty1, void * vctx ) {
+    DivCorrCtx & c = *static_cast<DivCorrCtx *>( vctx );
+    HGrid & E = *c.E;
+    HGrid & B = *c.B;
     const TileGeom & g = E.g;
     const int ys = E.extx;
-    const double dx_dy = ( (double) dx[0] ) / ( (double) dx[1] );
+    const double dx_dy = c.dx_dy;
     std::vector<double> divEx( g.nxy ), divBx( g.nxy );
-    for ( int ty = 0; ty < g.nty; ty++ ) {
+    for ( int ty = ty0; ty < ty1; ty++ ) {
         std::fill( divEx.begin(), divEx.end(), 0.0 );
         std::fill( divBx.begin(), divBx.end(), 0.0 );
         for ( int tx = g.ntx - 1; tx >= 0; tx-- ) {
@@ -373,30 +379,28 @@ void div_corr_x( HGrid & E, HGrid & B, const float dx[2] ) {
         }
     }
 }
-}  // namespace
 
-int laser_fields( zpic_laser_desc l, const TileGeom & g, const float box[2],
-                  std::vector<float> & Ev, std::vector<float> & Bv ) {
-    // Laser::Pulse::validate (laser.cpp:174-207), Gaussian::validate (299-310)
-    if ( l.a0 <= 0 || l.omega0 <= 0 ) return -1;
-    if ( l.fwhm > 0 ) { l.rise = l.fwhm; l.fall = l.fwhm; l.flat = 0.f; }
-    else if ( l.rise <= 0 || l.flat < 0 || l.fall <= 0 ) return -1;
-    if ( l.type == ZPIC_LASER_GAUSSIAN && l.W0 <= 0 ) return -1;
-    if ( l.cos_pol == 0 && l.sin_pol == 0 ) {
-        l.cos_pol = std::cos( l.polarization );
-        l.sin_pol = std::sin( l.polarization );
-    }
-    HGrid E{ g, GL + g.nxx + GU, GL + g.nxy + GU, 0, 0, &Ev };
-    E.off = GL * E.extx + GL;
-    E.tv = ( E.extx * E.exty + 3 ) & ~3;
-    HGrid B = E; B.buf = &Bv;
-    Ev.assign( (size_t) E.tv * g.ntiles() * 3, 0.f );
-    Bv.assign( (size_t) E.tv * g.ntiles() * 3, 0.f );
-    const float dx[2] = { box[0] / ( g.nxx * g.ntx ), box[1] / ( g.nxy * g.nty ) };
+void div_corr_x( HGrid & E, HGrid & B, const float dx[2] ) {
+    DivCorrCtx c{ &E, &B, ( (double) dx[0] ) / ( (double) dx[1] ) };
+    parallel_for( E.g.nty, div_corr_rows, &c );
+}
+
+// The pulse's fields, cell by cell (laser.cpp:233-292 plane wave,
+// 361-443 Gaussian), for tiles [t0, t1): every value depends on its own cell
+// only, so tiles are spread over host threads.
+struct PulseCtx { const zpic_laser_desc * l; HGrid * E; HGrid * B; float dx[2]; };
+
+void pulse_tiles( int t0, int t1, void * vctx ) {
+    PulseCtx & c = *static_cast<PulseCtx *>( vctx );
+    const zpic_laser_desc & l = *c.l;
+    HGrid & E = *c.E;
+    HGrid & B = *c.B;
+    const TileGeom & g = E.g;
+    const float * dx = c.dx;
     const int ys = E.extx;
     const float amp = l.omega0 * l.a0;
-    for ( int ty = 0; ty < g.nty; ty++ ) for ( int tx = 0; tx < g.ntx; tx++ ) {
-        const int tid = ty * g.ntx + tx;
+    for ( int tid = t0; tid < t1; tid++ ) {
+        const int tx = tid % g.ntx, ty = tid / g.ntx;
         float * pE = E.cell( tid, E.off );
         float * pB = B.cell( tid, B.off );
         const int ix0 = tx * g.nxx, iy0 = ty * g.nxy;
@@ -423,6 +427,29 @@ int laser_fields( zpic_laser_desc l, const TileGeom & g, const float box[2],
                 }
             }
     }
+}
+}  // namespace
+
+int laser_fields( zpic_laser_desc l, const TileGeom & g, const float box[2],
+                  std::vector<float> & Ev, std::vector<float> & Bv ) {
+    // Laser::Pulse::validate (laser.cpp:174-207), Gaussian::validate (299-310)
+    if ( l.a0 <= 0 || l.omega0 <= 0 ) return -1;
+    if ( l.fwhm > 0 ) { l.rise = l.fwhm; l.fall = l.fwhm; l.flat = 0.f; }
+    else if ( l.rise <= 0 || l.flat < 0 || l.fall <= 0 ) return -1;
+    if ( l.type == ZPIC_LASER_GAUSSIAN && l.W0 <= 0 ) return -1;
+    if ( l.cos_pol == 0 && l.sin_pol == 0 ) {
+        l.cos_pol = std::cos( l.polarization );
+        l.sin_pol = std::sin( l.polarization );
+    }
+    HGrid E{ g, GL + g.nxx + GU, GL + g.nxy + GU, 0, 0, &Ev };
+    E.off = GL * E.extx + GL;
+    E.tv = ( E.extx * E.exty + 3 ) & ~3;
+    HGrid B = E; B.buf = &Bv;
+    Ev.assign( (size_t) E.tv * g.ntiles() * 3, 0.f );
+    Bv.assign( (size_t) E.tv * g.ntiles() * 3, 0.f );
+    const float dx[2] = { box[0] / ( g.nxx * g.ntx ), box[1] / ( g.nxy * g.nty ) };
+    PulseCtx pc{ &l, &E, &B, { dx[0], dx[1] } };
+    parallel_for( g.ntiles(), pulse_tiles, &pc );
     copy_to_gc( E, 3 );
     copy_to_gc( B, 3 );
     if ( l.filter > 0 ) {
