@@ -43,16 +43,24 @@ def test_reorder_keeps_particles():
         a.set_option('reorder', -1)
 
 
-def test_reorder_round_robin_order():
-    s = weibel(zb.Simulation(*GEOM))
+@pytest.mark.parametrize('nx, ppc', [((16, 16), (4, 4)), ((16, 16), (9, 9)), ((32, 32), (2, 2))])
+def test_reorder_round_robin_order(nx, ppc):
+    """Both launch forms: two 512-thread CTAs per SM for 16x16 tiles that fit
+    half of the shared memory, one 1024-thread CTA for larger tiles (16x16
+    cells at 81 per cell: 20,736 particles) and for tiles of more cells."""
+    geom = ((64 // nx[0], 64 // nx[1]), nx, (6.4, 6.4), 0.07)
+    s = zb.Simulation(*geom)
+    s.add_species(-1.0, ppc, udist=('thermalcorr', (0.1, 0.1, 0.1), (0, 0, 0.6)))
+    s.add_species(1.0, ppc, udist=('thermalcorr', (0.1, 0.1, 0.1), (0, 0, -0.6)))
     s.set_option('reorder', 5)
     s.advance(5)                       # the last thing step 5 does is a reorder
     for sp in range(2):
         npt, ix, x, u = s.particles(sp)
+        assert int(npt.max()) > 64
         o = 0
         for n in npt:
-            cell = ix[o:o + n, 0] + 16 * ix[o:o + n, 1]
-            counts = np.bincount(cell, minlength=256)
+            cell = ix[o:o + n, 0] + nx[0] * ix[o:o + n, 1]
+            counts = np.bincount(cell, minlength=nx[0] * nx[1])
             # round r holds one particle of each cell with more than r
             # particles, in ascending cell order
             k = 0

@@ -114,7 +114,7 @@ enum Phase { PH_PARTICLES = 0, PH_SORT, PH_CURRENT, PH_FIELDS, PH_OTHER, PH_N };
 // there the plasma is cold and new particles arrive in injection order every
 // step, so the order hardly decays.  On the uniform plasma the particle
 // kernel takes 4.56 ms per step right after a reorder and 4.95 ms a hundred
-// steps later; a reorder costs ~4 ms, 0.08 ms per step at this interval.
+// steps later; a reorder costs ~3.9 ms, 0.08 ms per step at this interval.
 constexpr int REORDER_DEFAULT = -1;
 constexpr int REORDER_AUTO_STEPS = 50;
 

@@ -1518,20 +1518,22 @@ __global__ void k_np_stats( const SpDev * __restrict__ sps, int sp, unsigned lon
 // so round r lists one particle of every cell that holds more than r, in
 // ascending cell order, and consecutive lanes again see consecutive cells.
 // The rank comes from a shared-memory counter per cell (its order between
-// particles of one cell is arbitrary; the ranks stay in shared memory, beside
-// the tile's cells, which are read once); the position of (r, c) is the number of
-// particles in the rounds before r plus the cells before c in round r,
-// counted with a bit mask of the cells present in each round.  The tile is
-// then permuted in place one particle array at a time through shared memory
-// (coalesced loads and stores, 8 bytes of traffic per particle and array).
-// One CTA per tile; tiles with more particles than fit in shared memory, with
-// more particles in one cell than there are rounds, or with a particle outside
-// the tile are left as they are.
-constexpr int RO_THREADS = 1024;
-
-__global__ void __launch_bounds__( RO_THREADS, 1 )
+// particles of one cell is arbitrary) and is kept beside the cell index in
+// the shared copy of the tile's cells, which are read once; the position of
+// (r, c) is the number of particles in the rounds before r plus the cells
+// before c in round r, counted with a bit mask of the cells present in each
+// round.  The tile is then permuted in place one particle array at a time
+// through shared memory (coalesced loads and stores, 8 bytes of traffic per
+// particle and array; the cell words are rebuilt from the cell indices).
+// One CTA per tile, either 1024 threads alone on an SM or, for tiles that
+// fit half of the shared memory, 512 threads with two CTAs per SM (one
+// CTA's loads and stores overlap the other's counting).  Tiles with more
+// particles than fit, with more particles in one cell than there are rounds,
+// or with a particle outside the tile are left as they are.
+template < int NT >
+__global__ void __launch_bounds__( NT, 1024 / NT )
 k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, const RunDev * __restrict__ runs,
-           int max_rounds, int np_max )
+           int max_rounds, int np_min, int np_max )
 {
     extern __shared__ __align__( 16 ) unsigned char smem_raw[];
     const Item it = items[ blockIdx.x ];
@@ -1539,16 +1541,15 @@ k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, cons
     const RunDev & R = runs[ S.run ];
     const int t = it.tile;
     const int np = S.np[t];
-    if ( np < 64 || np > np_max ) return;
+    if ( np < np_min || np > np_max ) return;
     const size_t off = S.off[t];
     const int nxx = R.nxx, nxy = R.nxy, ncell = nxx * nxy;
     const int ncw = ( ncell + 31 ) >> 5;
-    // shared memory: [buf: np_max words][inv: np_max 16-bit][rank: np_max 16-bit][cnt: ncw*32]
+    // shared memory: [buf: np_max words][inv: np_max 16-bit][cnt: ncw*32]
     //                [base: max_rounds+1][flags: 4][masks: max_rounds*ncw words][word prefix: max_rounds*ncw 16-bit]
     uint32_t * buf = reinterpret_cast<uint32_t *>( smem_raw );
     uint16_t * inv = reinterpret_cast<uint16_t *>( buf + np_max );
-    uint16_t * rank = inv + np_max;
-    int * cnt = reinterpret_cast<int *>( rank + np_max );
+    int * cnt = reinterpret_cast<int *>( inv + np_max );
     int * base = cnt + ncw * 32;
     int * flags = base + max_rounds + 1;
     uint32_t * masks = reinterpret_cast<uint32_t *>( flags + 4 );
@@ -1558,28 +1559,31 @@ k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, cons
     // the tile's cells, read once into shared memory
     {
         const uint32_t * g = S.A.cell + off;
-        for ( int v = threadIdx.x; v < n4; v += blockDim.x )
+#pragma unroll 4
+        for ( int v = threadIdx.x; v < n4; v += NT )
             reinterpret_cast<uint4 *>( buf )[v] = reinterpret_cast<const uint4 *>( g )[v];
-        for ( int p = 4 * n4 + threadIdx.x; p < np; p += blockDim.x ) buf[p] = g[p];
+        for ( int p = 4 * n4 + threadIdx.x; p < np; p += NT ) buf[p] = g[p];
     }
-    for ( int c = threadIdx.x; c < ncw * 32; c += blockDim.x ) cnt[c] = 0;
+    for ( int c = threadIdx.x; c < ncw * 32; c += NT ) cnt[c] = 0;
     if ( threadIdx.x == 0 ) { flags[0] = 0; flags[1] = 0; }
     __syncthreads();
-    for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
+    // rank within the cell, kept as (cell index | rank << 16)
+    for ( int i = threadIdx.x; i < np; i += NT ) {
         const uint32_t cl = buf[i];
         const int ix = cell_x( cl ), iy = cell_y( cl );
         if ( ix < 0 || ix >= nxx || iy < 0 || iy >= nxy ) { flags[0] = 1; continue; }
-        const int r = atomicAdd( cnt + ix + nxx * iy, 1 );
-        rank[i] = (uint16_t) r;
+        const int c = ix + nxx * iy;
+        const int r = atomicAdd( cnt + c, 1 );
         if ( r >= max_rounds ) flags[0] = 1;
-        else atomicMax( flags + 1, r + 1 );
+        else { atomicMax( flags + 1, r + 1 ); buf[i] = (uint32_t) c | ( (uint32_t) r << 16 ); }
     }
     __syncthreads();
     if ( flags[0] ) return;
     const int nround = flags[1];
     // cells present in each round, one 32-cell word per warp pass
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for ( int w = warp; w < ncw; w += nwarp ) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
+    for ( int w = warp; w < ncw; w += NW ) {
         const int n = cnt[ w * 32 + lane ];
         for ( int r = 0; r < nround; r++ ) {
             const uint32_t m = __ballot_sync( 0xffffffffu, n > r );
@@ -1588,7 +1592,7 @@ k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, cons
     }
     __syncthreads();
     // per round: prefix of the word populations, and the round's size
-    for ( int r = threadIdx.x; r < nround; r += blockDim.x ) {
+    for ( int r = threadIdx.x; r < nround; r += NT ) {
         int a = 0;
         for ( int w = 0; w < ncw; w++ ) { wpre[ r * ncw + w ] = (uint16_t) a; a += __popc( masks[ r * ncw + w ] ); }
         base[r] = a;
@@ -1611,32 +1615,50 @@ k_reorder( const Item * __restrict__ items, const SpDev * __restrict__ sps, cons
         }
     }
     __syncthreads();
-    for ( int i = threadIdx.x; i < np; i += blockDim.x ) {
-        const uint32_t cl = buf[i];
-        const int c = cell_x( cl ) + nxx * cell_y( cl );
-        const int r = rank[i];
+    for ( int i = threadIdx.x; i < np; i += NT ) {
+        const uint32_t e = buf[i];
+        const int c = e & 0xffff, r = e >> 16;
         const int w = c >> 5;
         const int pos = base[r] + wpre[ r * ncw + w ] + __popc( masks[ r * ncw + w ] & ( ( 1u << ( c & 31 ) ) - 1u ) );
         inv[pos] = (uint16_t) i;
     }
-    // permute each particle array in place through shared memory
-    uint32_t * arr[6] = { S.A.cell, reinterpret_cast<uint32_t *>( S.A.xx ), reinterpret_cast<uint32_t *>( S.A.xy ),
+    __syncthreads();
+    // the cells, rebuilt from the cell indices
+    {
+        uint32_t * g = S.A.cell + off;
+#pragma unroll 4
+        for ( int v = threadIdx.x; v < n4; v += NT ) {
+            uint32_t q[4];
+#pragma unroll
+            for ( int u = 0; u < 4; u++ ) {
+                const int c = buf[ inv[ 4 * v + u ] ] & 0xffff;
+                q[u] = pack_cell( c % nxx, c / nxx );
+            }
+            reinterpret_cast<uint4 *>( g )[v] = make_uint4( q[0], q[1], q[2], q[3] );
+        }
+        for ( int p = 4 * n4 + threadIdx.x; p < np; p += NT ) {
+            const int c = buf[ inv[p] ] & 0xffff;
+            g[p] = pack_cell( c % nxx, c / nxx );
+        }
+    }
+    // then each other particle array in place through shared memory
+    uint32_t * arr[5] = { reinterpret_cast<uint32_t *>( S.A.xx ), reinterpret_cast<uint32_t *>( S.A.xy ),
                           reinterpret_cast<uint32_t *>( S.A.ux ), reinterpret_cast<uint32_t *>( S.A.uy ),
                           reinterpret_cast<uint32_t *>( S.A.uz ) };
-    for ( int a = 0; a < 6; a++ ) {
+    for ( int a = 0; a < 5; a++ ) {
         uint32_t * g = arr[a] + off;
         __syncthreads();
-        if ( a > 0 ) {                            // the cells are in buf already
-            for ( int v = threadIdx.x; v < n4; v += blockDim.x )
-                reinterpret_cast<uint4 *>( buf )[v] = reinterpret_cast<const uint4 *>( g )[v];
-            for ( int p = 4 * n4 + threadIdx.x; p < np; p += blockDim.x ) buf[p] = g[p];
-            __syncthreads();
-        }
-        for ( int v = threadIdx.x; v < n4; v += blockDim.x ) {
+#pragma unroll 4
+        for ( int v = threadIdx.x; v < n4; v += NT )
+            reinterpret_cast<uint4 *>( buf )[v] = reinterpret_cast<const uint4 *>( g )[v];
+        for ( int p = 4 * n4 + threadIdx.x; p < np; p += NT ) buf[p] = g[p];
+        __syncthreads();
+#pragma unroll 4
+        for ( int v = threadIdx.x; v < n4; v += NT ) {
             const int p = 4 * v;
             reinterpret_cast<uint4 *>( g )[v] = make_uint4( buf[ inv[p] ], buf[ inv[p + 1] ], buf[ inv[p + 2] ], buf[ inv[p + 3] ] );
         }
-        for ( int p = 4 * n4 + threadIdx.x; p < np; p += blockDim.x ) g[p] = buf[ inv[p] ];
+        for ( int p = 4 * n4 + threadIdx.x; p < np; p += NT ) g[p] = buf[ inv[p] ];
     }
 }
 
@@ -1783,22 +1805,43 @@ cudaError_t launch_energy_sum( cudaStream_t st, const SpDev * sps, int sp, int n
 }
 
 // Rounds (the most particles in one cell) and particles per tile that
-// k_reorder handles for tiles of up to max_cells cells, within 227 KB of
-// shared memory.
+// k_reorder handles for tiles of up to max_cells cells: 1024 threads in
+// 227 KB of shared memory, or two CTAs of 512 threads per SM in 113 KB each
+// (tiles of up to 256 cells with fewer particles than fit there; the large
+// configuration takes the larger tiles in a second launch).
 cudaError_t launch_reorder( cudaStream_t st, const Item * items, int nitems, const SpDev * sps, const RunDev * runs,
                             int max_cells ) {
     if ( nitems <= 0 ) return cudaSuccess;
     const int ncw = ( max_cells + 31 ) / 32;
+    auto fixed_bytes = [&]( int rounds ) {
+        return (size_t) ncw * 32 * 4 + ( rounds + 1 ) * 4 + 16 + (size_t) rounds * ncw * 6;
+    };
+    // per particle: one 4-byte word (the cells with their ranks, then the
+    // array being permuted) and a 16-bit source index
+    auto np_fit = [&]( size_t budget, int rounds ) -> int {
+        const size_t fx = fixed_bytes( rounds );
+        if ( fx + 64 * 6 > budget ) return 0;
+        return (int) std::min<size_t>( 65532, ( ( budget - fx ) / 6 ) & ~(size_t) 7 );
+    };
+    int np_lo = 64;
+    if ( max_cells <= 256 ) {
+        const int rounds = 127;
+        const int np2 = np_fit( 113 * 1024, rounds );
+        if ( np2 >= 1024 ) {
+            const size_t smem = (size_t) np2 * 6 + fixed_bytes( rounds );
+            cudaFuncSetAttribute( (const void *) k_reorder<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
+            k_reorder<512><<< nitems, 512, smem, st >>>( items, sps, runs, rounds, np_lo, np2 );
+            const cudaError_t e = cudaGetLastError();
+            if ( e != cudaSuccess ) return e;
+            np_lo = np2 + 1;
+        }
+    }
     const int rounds = std::max( 1, std::min( 511, ( 32 * 1024 ) / ( 6 * ncw ) - 1 ) );
-    const size_t fixed = (size_t) ncw * 32 * 4 + ( rounds + 1 ) * 4 + 16 + (size_t) rounds * ncw * 6;
-    const size_t budget = 227 * 1024;
-    if ( fixed + 64 * 8 > budget ) return cudaSuccess;
-    // per particle: one 4-byte word of the array being permuted, a 16-bit
-    // source index and a 16-bit rank
-    const int np_max = std::min<size_t>( 65532, ( ( budget - fixed ) / 8 ) & ~(size_t) 7 );
-    const size_t smem = (size_t) np_max * 8 + fixed;
-    cudaFuncSetAttribute( (const void *) k_reorder, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
-    k_reorder<<< nitems, RO_THREADS, smem, st >>>( items, sps, runs, rounds, np_max );
+    const int np1 = np_fit( 227 * 1024, rounds );
+    if ( np1 < np_lo ) return cudaSuccess;
+    const size_t smem = (size_t) np1 * 6 + fixed_bytes( rounds );
+    cudaFuncSetAttribute( (const void *) k_reorder<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
+    k_reorder<1024><<< nitems, 1024, smem, st >>>( items, sps, runs, rounds, np_lo, np1 );
     return cudaGetLastError();
 }
 
