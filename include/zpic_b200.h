@@ -160,10 +160,11 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  *                         contributions rounded to 2^-29 |q| and summed exactly
  *                         in integer arithmetic, independent of the order of
  *                         the additions; the fastest of the three)
- *   "reorder"        n    every n steps, put each tile's particles back into
- *                         cell round-robin order (one particle of every cell,
- *                         cells ascending, then the next round), which keeps
- *                         the particle kernel's shared-memory bank conflicts at
+ *   "reorder"        n    every n steps, put the particles of every window
+ *                         of 1024 slots of a tile back into cell round-robin
+ *                         order (one particle of every cell present, cells
+ *                         ascending, then the next round), which keeps the
+ *                         particle kernel's shared-memory bank conflicts at
  *                         their initial level; 0 never.  Default: every 50
  *                         steps, never in a moving-window run.  Order only:
  *                         every tile keeps its particle multiset.
@@ -293,8 +294,8 @@ int zpic_b200_grid_gather( zpic_sim * sim, int32_t which, int32_t fc, float * ou
  * queued (ZPIC_E_INVALID otherwise): a tile block of (nx_x+1)*(nx_y+1) cells
  * at most 12288, and ntiles_x*ntiles_y * roundup4((nx_x+1)*(nx_y+1)) at most
  * 8 Mi floats.  The first call on a device (and the first after that
- * device's context was reset) resolves the array's address on that device;
- * make that first call before any stream capture.  All calls share the
+ * device's context was reset) resolves the array's address on that device
+ * with a host-side lookup.  All calls share the
  * array, which keeps the last call's contents (each call clears the part it
  * uses): calls that overlap on the GPU race and must be serialised.
  */
