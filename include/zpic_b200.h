@@ -160,11 +160,10 @@ int zpic_b200_sim_synchronize( zpic_sim * sim );
  *                         contributions rounded to 2^-29 |q| and summed exactly
  *                         in integer arithmetic, independent of the order of
  *                         the additions; the fastest of the three)
- *   "reorder"        n    every n steps, put the particles of every window
- *                         of 1024 slots of a tile back into cell round-robin
- *                         order (one particle of every cell present, cells
- *                         ascending, then the next round), which keeps the
- *                         particle kernel's shared-memory bank conflicts at
+ *   "reorder"        n    every n steps, put each tile's particles back into
+ *                         cell round-robin order (one particle of every cell,
+ *                         cells ascending, then the next round), which keeps
+ *                         the particle kernel's shared-memory bank conflicts at
  *                         their initial level; 0 never.  Default: every 50
  *                         steps, never in a moving-window run.  Order only:
  *                         every tile keeps its particle multiset.
