@@ -471,25 +471,33 @@ k_kernel3( const TileItem * __restrict__ items, const RunDev * __restrict__ runs
 }
 
 // grid::x_shift_left(1) data motion on E and B (grid.h:455-485); the x guard
-// refresh follows as a separate k_emf_gc( axes = 1 ) launch.
-__global__ void __launch_bounds__( 128 )
+// refresh follows as a separate k_emf_gc( axes = 1 ) launch.  Both fields'
+// tile blocks are staged in shared memory with 16-byte loads in one pass
+// (3 tile_vol floats per field, a multiple of 4), then written back shifted
+// by one cell, the last cell of every row cleared.
+constexpr int SHIFT_THREADS = 256;
+
+__global__ void __launch_bounds__( SHIFT_THREADS )
 k_shift_left( const TileItem * __restrict__ items, const RunDev * __restrict__ runs )
 {
-    extern __shared__ float sA[];
+    extern __shared__ __align__( 16 ) float sA[];   // [E block][B block]
     const TileItem it = items[ blockIdx.x ];
     const RunDev & R = runs[ it.run ];
-    const int n = 3 * R.tile_vol;
-    const int ys = R.extx;
-    for ( int f = 0; f < 2; f++ ) {
-        float * g = ( f == 0 ? R.E : R.B ) + (size_t) it.tile * R.tile_vol * 3;
-        for ( int i = threadIdx.x; i < n; i += blockDim.x ) sA[i] = g[i];
-        __syncthreads();
-        for ( int q = threadIdx.x; q < R.extx * R.exty; q += blockDim.x ) {
-            const int ix = q % ys, iy = q / ys;
-            for ( int k = 0; k < 3; k++ )
-                g[ 3 * q + k ] = ( ix < ys - 1 ) ? sA[ 3 * ( ix + 1 + iy * ys ) + k ] : 0.0f;
-        }
-        __syncthreads();
+    const int n = 3 * R.tile_vol, n4 = n >> 2;
+    float * gE = R.E + (size_t) it.tile * n;
+    float * gB = R.B + (size_t) it.tile * n;
+#pragma unroll 4
+    for ( int v = threadIdx.x; v < 2 * n4; v += SHIFT_THREADS ) {
+        const float4 * src = reinterpret_cast<const float4 *>( v < n4 ? gE : gB );
+        reinterpret_cast<float4 *>( sA )[v] = src[ v < n4 ? v : v - n4 ];
+    }
+    __syncthreads();
+    const int ys = R.extx, nc = 3 * R.extx * R.exty;
+#pragma unroll 4
+    for ( int f = threadIdx.x; f < 2 * nc; f += SHIFT_THREADS ) {
+        const int fld = f >= nc, e = f - fld * nc;    // float e of cell e / 3 in the field's block
+        const int ix = ( e / 3 ) % ys;
+        ( fld ? gB : gE )[e] = ( ix < ys - 1 ) ? sA[ fld * n + e + 3 ] : 0.0f;
     }
 }
 
@@ -620,9 +628,9 @@ cudaError_t launch_kernel3( cudaStream_t st, const TileItem * items, int n, cons
     return cudaGetLastError();
 }
 cudaError_t launch_shift_left( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int max_tile_vol ) {
-    const size_t smem = (size_t) 3 * max_tile_vol * sizeof( float );
+    const size_t smem = (size_t) 6 * max_tile_vol * sizeof( float );
     if ( smem > 48 * 1024 ) cudaFuncSetAttribute( (const void *) k_shift_left, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
-    if ( n > 0 ) k_shift_left<<< n, 128, smem, st >>>( items, runs );
+    if ( n > 0 ) k_shift_left<<< n, SHIFT_THREADS, smem, st >>>( items, runs );
     return cudaGetLastError();
 }
 cudaError_t launch_field_energy( cudaStream_t st, const RunDev * runs, int run, int ntiles, double * out ) {
