@@ -383,6 +383,27 @@ def test_moving_window_graph_replay():
     assert rel_err(ea[0].sum() + ea[1].sum(), eb[0].sum() + eb[1].sum()) <= 1e-5
 
 
+def test_window_shift_after_field_solve_bit_exact():
+    """In a moving-window step the window shift takes over the field solve's
+    guard-cell refresh (the Yee kernel keeps B's first interior column for
+    it).  Fields, guard cells included, must be bit for bit those of the
+    field solve and the shift issued one after the other with their own guard
+    refreshes (EMF::advance through emf_advance), over steps with and without
+    a move; random E and B, no particles (zero current)."""
+    geom = ((8, 4), (16, 16), (128 * 0.025, 64 * 0.1), 0.022)
+    a, b = zb.Simulation(*geom), zb.Simulation(*geom)
+    E, B = random_fields(a, 11), random_fields(a, 12)
+    for s in (a, b):
+        s.set_moving_window()
+        s.set_grid('E', E)
+        s.set_grid('B', B)
+    for n in range(8):
+        a.advance_mov_window(1)
+        b.emf_advance(True)
+        for w in 'EB':
+            assert np.array_equal(a.grid(w), b.grid(w)), 'step %d, %s' % (n + 1, w)
+
+
 @pytest.mark.parametrize('nx, chunks', [((8, 8), 0), ((32, 32), 0), ((16, 16), -1), ((24, 8), 3)])
 def test_tile_shapes_and_chunking(nx, chunks):
     """Tile shapes other than the compile-time 16x16 one, and the CTA

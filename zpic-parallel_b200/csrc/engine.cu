@@ -43,11 +43,11 @@ cudaError_t launch_reorder( cudaStream_t, const Item *, int, const SpDev *, cons
 cudaError_t launch_current_gc( cudaStream_t, const TileItem *, int, const RunDev *, int );
 cudaError_t launch_emf_gc( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
 cudaError_t launch_cur_gc( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
-cudaError_t launch_yee( cudaStream_t, const TileItem *, int, const RunDev *, int, int, int, int );
+cudaError_t launch_yee( cudaStream_t, const TileItem *, int, const RunDev *, int, int, int, int, int );
 cudaError_t launch_emf_bc( cudaStream_t, const RunDev *, int, int, int );
 cudaError_t launch_cur_bc( cudaStream_t, const RunDev *, int, int, int );
 cudaError_t launch_kernel3( cudaStream_t, const TileItem *, int, const RunDev *, int, int, float, float, float, int );
-cudaError_t launch_shift_left( cudaStream_t, const TileItem *, int, const RunDev *, int );
+cudaError_t launch_shift_left( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
 cudaError_t launch_field_energy( cudaStream_t, const RunDev *, int, int, double * );
 cudaError_t launch_grid_add( cudaStream_t, float *, const float *, size_t );
 cudaError_t launch_charge_finish( cudaStream_t, const float *, float *, int, int, int, int, int, int, int, int );
@@ -571,11 +571,19 @@ static int run_current( Plan & P, cudaStream_t st ) {
     return ZPIC_OK;
 }
 
-// EMF::advance device part (emf.cpp:513-580 and 135-194): Yee, guard cells, bc
-static int run_fields( Plan & P, cudaStream_t st, int with_j, int j_raw, int clear_jdep ) {
+// EMF::advance device part (emf.cpp:513-580 and 135-194): Yee, guard cells, bc.
+// before_shift: a window shift of a run without physical boundaries follows
+// at once; the Yee kernel saves the first interior column of B for it and
+// the guard refresh is left to the shift (run_shift's from_yee).
+static int run_fields( Plan & P, cudaStream_t st, int with_j, int j_raw, int clear_jdep, bool before_shift = false ) {
+    if ( before_shift ) {
+        PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 1 );
+        DEV( launch_yee( st, P.tile_items_d, P.n_tiles, P.runs_d, with_j, j_raw, clear_jdep, P.max_tile_vol, 1 ) );
+        return ZPIC_OK;
+    }
     {
         PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 2 );
-        DEV( launch_yee( st, P.tile_items_d, P.n_tiles, P.runs_d, with_j, j_raw, clear_jdep, P.max_tile_vol ) );
+        DEV( launch_yee( st, P.tile_items_d, P.n_tiles, P.runs_d, with_j, j_raw, clear_jdep, P.max_tile_vol, 0 ) );
         DEV( launch_emf_gc( st, P.tile_items_d, P.n_tiles, P.runs_d, 3, P.max_guard ) );
     }
     if ( !P.needs_bc_or_filter ) return ZPIC_OK;
@@ -593,14 +601,16 @@ static int run_fields( Plan & P, cudaStream_t st, int with_j, int j_raw, int cle
     return ZPIC_OK;
 }
 
-// EMF::move_window (emf.cpp:120-129) for one run of the plan
-static int run_shift( Plan & P, cudaStream_t st, int r ) {
+// EMF::move_window (emf.cpp:120-129) for one run of the plan.  from_yee:
+// straight after run_fields( ..., before_shift ), whose guard refresh the
+// shift's (both axes instead of x) replaces.
+static int run_shift( Plan & P, cudaStream_t st, int r, bool from_yee = false ) {
     int first = 0;
     for ( int q = 0; q < r; q++ ) first += P.sims[q]->ntx * P.sims[q]->nty;
     const int nt = P.sims[r]->ntx * P.sims[r]->nty;
     PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 2 );
-    DEV( launch_shift_left( st, P.tile_items_d + first, nt, P.runs_d, P.max_tile_vol ) );
-    DEV( launch_emf_gc( st, P.tile_items_d + first, nt, P.runs_d, 1, P.max_guard ) );
+    DEV( launch_shift_left( st, P.tile_items_d + first, nt, P.runs_d, P.max_tile_vol, from_yee ? 1 : 0 ) );
+    DEV( launch_emf_gc( st, P.tile_items_d + first, nt, P.runs_d, from_yee ? 3 : 1, P.max_guard ) );
     return ZPIC_OK;
 }
 
@@ -1253,6 +1263,7 @@ int zpic_b200_sim_create( uint32_t ntx, uint32_t nty, uint32_t nxx, uint32_t nxy
     R.dt = (float) dt;
     const size_t nf = s->grid_floats();
     TRY( dalloc( &R.E, nf ) ); TRY( dalloc( &R.B, nf ) ); TRY( dalloc( &R.J, nf ) ); TRY( dalloc( &R.Jdep, nf ) );
+    TRY( dalloc( &R.bcol, (size_t) ntx * nty * nxy * 3 ) );
     CK( cudaMemset( R.E, 0, nf * sizeof( float ) ) );
     CK( cudaMemset( R.B, 0, nf * sizeof( float ) ) );
     CK( cudaMemset( R.J, 0, nf * sizeof( float ) ) );
@@ -1282,7 +1293,7 @@ int zpic_b200_sim_destroy( zpic_sim * s ) {
     resolve_phase_events( s );
     s->plan.release();
     for ( auto * sp : s->species ) { sp->free_all(); delete sp; }
-    dfree( s->run.E ); dfree( s->run.B ); dfree( s->run.J ); dfree( s->run.Jdep );
+    dfree( s->run.E ); dfree( s->run.B ); dfree( s->run.J ); dfree( s->run.Jdep ); dfree( s->run.bcol );
     dfree( s->status ); dfree( s->dscratch ); dfree( s->shifts_d ); dfree( s->fe_part_d );
     if ( s->fe_part_h ) { cudaFreeHost( s->fe_part_h ); s->fe_part_h = nullptr; }
     if ( s->hscratch ) cudaFreeHost( s->hscratch );
@@ -1477,12 +1488,19 @@ static int mw_step( zpic_sim * s ) {
     TRY( run_current( P, P.side ) );
     s->cur_iter++;
     if ( s->cur_mw.needs_move( s->cur_iter * s->dt ) ) s->cur_mw.advance();
-    TRY( run_fields( P, P.side, 1, 0, 1 ) );
+    // a window shift right after the field solve takes over its guard refresh
+    // when no physical boundary has to be applied in between and every y
+    // guard cell has a source (periodic y): then the guard cells come out
+    // the same as with the two refreshes
+    const bool shift = s->emf_mw.active && s->emf_mw.needs_move( ( s->emf_iter + 1 ) * s->dt );
+    bool fused = shift && P.sims.size() == 1 && s->run.emf_pery;
+    for ( int k = 0; k < 4; k++ ) fused = fused && s->emf_bc[k] <= ZPIC_EMF_BC_PERIODIC;
+    TRY( run_fields( P, P.side, 1, 0, 1, fused ) );
     s->jdep_clean = true;
     s->j_final = true;
     s->emf_iter++;
-    if ( s->emf_mw.active && s->emf_mw.needs_move( s->emf_iter * s->dt ) ) {
-        TRY( run_shift( P, P.side, 0 ) );
+    if ( shift ) {
+        TRY( run_shift( P, P.side, 0, fused ) );
         s->emf_mw.advance();
     }
     DEV( cudaEventRecord( P.join, P.side ) );

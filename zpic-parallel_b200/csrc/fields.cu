@@ -216,7 +216,8 @@ __device__ __forceinline__ void yee_e_smem( float * E, const float * B, const fl
 }
 
 __global__ void __launch_bounds__( YEE_THREADS )
-k_yee( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, int with_j, int j_raw, int clear_jdep )
+k_yee( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, int with_j, int j_raw, int clear_jdep,
+       int save_bcol )
 {
     extern __shared__ __align__( 16 ) unsigned char smem_raw[];
     const TileItem it = items[ blockIdx.x ];
@@ -260,6 +261,12 @@ k_yee( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, in
     if ( clear_jdep ) {
         float4 * z = reinterpret_cast<float4 *>( R.Jdep + toff );
         for ( int i = threadIdx.x; i < 3 * tv / 4; i += blockDim.x ) z[i] = make_float4( 0.f, 0.f, 0.f, 0.f );
+    }
+    if ( save_bcol ) {
+        // B of the first interior column, for the window shift that follows
+        // (the left neighbour's new last interior column)
+        float * dst = R.bcol + (size_t) it.tile * R.nxy * 3;
+        for ( int q = threadIdx.x; q < 3 * R.nxy; q += blockDim.x ) dst[q] = B0[ 3 * ( ( q / 3 ) * R.extx ) + q % 3 ];
     }
     // the shared-memory sources read; the stores complete before the kernel does
     if ( threadIdx.x == 0 ) bulk_wait_read_all();
@@ -478,7 +485,7 @@ k_kernel3( const TileItem * __restrict__ items, const RunDev * __restrict__ runs
 constexpr int SHIFT_THREADS = 256;
 
 __global__ void __launch_bounds__( SHIFT_THREADS )
-k_shift_left( const TileItem * __restrict__ items, const RunDev * __restrict__ runs )
+k_shift_left( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, int from_yee )
 {
     extern __shared__ __align__( 16 ) float sA[];   // [E block][B block]
     const TileItem it = items[ blockIdx.x ];
@@ -493,6 +500,24 @@ k_shift_left( const TileItem * __restrict__ items, const RunDev * __restrict__ r
     }
     __syncthreads();
     const int ys = R.extx, nc = 3 * R.extx * R.exty;
+    if ( from_yee ) {
+        // Straight after the Yee kernel, before any guard refresh.  The new
+        // last interior column takes the first upper guard column: E there is
+        // the Yee kernel's own update of that column, bit for bit the right
+        // neighbour's (same inputs, same arithmetic), but B there needs E one
+        // column further out, so B's guard column is replaced by the right
+        // neighbour's saved first interior column (bcol); without a right
+        // neighbour the guard is kept, as a guard refresh would.  Every guard
+        // cell is refreshed afterwards (axes 3).
+        const int tx = it.tile % R.ntx, ty = it.tile / R.ntx;
+        const int rn = tx + 1 < R.ntx ? tx + 1 : ( R.emf_perx ? 0 : -1 );
+        if ( rn >= 0 ) {
+            const float * src = R.bcol + (size_t) ( ty * R.ntx + rn ) * R.nxy * 3;
+            for ( int q = threadIdx.x; q < 3 * R.nxy; q += SHIFT_THREADS )
+                sA[ n + 3 * ( ( q / 3 + 1 ) * ys + R.nxx + 1 ) + q % 3 ] = src[q];
+            __syncthreads();
+        }
+    }
 #pragma unroll 4
     for ( int f = threadIdx.x; f < 2 * nc; f += SHIFT_THREADS ) {
         const int fld = f >= nc, e = f - fld * nc;    // float e of cell e / 3 in the field's block
@@ -606,10 +631,10 @@ cudaError_t launch_cur_gc( cudaStream_t st, const TileItem * items, int n, const
     return cudaGetLastError();
 }
 cudaError_t launch_yee( cudaStream_t st, const TileItem * items, int n, const RunDev * runs,
-                        int with_j, int j_raw, int clear_jdep, int max_tile_vol ) {
+                        int with_j, int j_raw, int clear_jdep, int max_tile_vol, int save_bcol ) {
     const size_t smem = yee_smem_bytes( max_tile_vol );
     if ( smem > 48 * 1024 ) cudaFuncSetAttribute( (const void *) k_yee, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
-    if ( n > 0 ) k_yee<<< n, YEE_THREADS, smem, st >>>( items, runs, with_j, j_raw, clear_jdep );
+    if ( n > 0 ) k_yee<<< n, YEE_THREADS, smem, st >>>( items, runs, with_j, j_raw, clear_jdep, save_bcol );
     return cudaGetLastError();
 }
 cudaError_t launch_emf_bc( cudaStream_t st, const RunDev * runs, int run, int axis, int nthreads ) {
@@ -627,10 +652,11 @@ cudaError_t launch_kernel3( cudaStream_t st, const TileItem * items, int n, cons
     if ( n > 0 ) k_kernel3<<< n, 128, smem, st >>>( items, runs, which, diry, a, b, c );
     return cudaGetLastError();
 }
-cudaError_t launch_shift_left( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int max_tile_vol ) {
+cudaError_t launch_shift_left( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int max_tile_vol,
+                               int from_yee ) {
     const size_t smem = (size_t) 6 * max_tile_vol * sizeof( float );
     if ( smem > 48 * 1024 ) cudaFuncSetAttribute( (const void *) k_shift_left, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
-    if ( n > 0 ) k_shift_left<<< n, SHIFT_THREADS, smem, st >>>( items, runs );
+    if ( n > 0 ) k_shift_left<<< n, SHIFT_THREADS, smem, st >>>( items, runs, from_yee );
     return cudaGetLastError();
 }
 cudaError_t launch_field_energy( cudaStream_t st, const RunDev * runs, int run, int ntiles, double * out ) {

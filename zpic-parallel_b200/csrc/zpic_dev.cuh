@@ -32,6 +32,8 @@ struct RunDev {
     float * E; float * B;         // float3 per cell
     float * J;                    // final current (after guard-cell exchange)
     float * Jdep;                 // raw deposits (tile-local sums incl. guard cells)
+    float * bcol;                 // B of every tile's first interior column (ntiles x nxy float3),
+                                  // saved by the Yee kernel ahead of a window shift
     int emf_perx, emf_pery;       // E/B periodic flags (grid::periodic)
     int cur_perx, cur_pery;       // J periodic flags
     float dtx, dty, dtx2, dty2;   // Yee coefficients dt/dx, dt/dy and halves (emf.cpp:524-525)
