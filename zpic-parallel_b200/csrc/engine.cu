@@ -41,13 +41,13 @@ cudaError_t launch_energy_sum( cudaStream_t, const SpDev *, int, int, double * )
 cudaError_t launch_np_stats( cudaStream_t, const SpDev *, int, unsigned long long * );
 cudaError_t launch_reorder( cudaStream_t, const Item *, int, const SpDev *, const RunDev *, int );
 cudaError_t launch_current_gc( cudaStream_t, const TileItem *, int, const RunDev *, int );
-cudaError_t launch_emf_gc( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
+cudaError_t launch_emf_gc( cudaStream_t, const TileItem *, int, const RunDev *, int, int, int );
 cudaError_t launch_cur_gc( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
 cudaError_t launch_yee( cudaStream_t, const TileItem *, int, const RunDev *, int, int, int, int, int );
 cudaError_t launch_emf_bc( cudaStream_t, const RunDev *, int, int, int );
 cudaError_t launch_cur_bc( cudaStream_t, const RunDev *, int, int, int );
 cudaError_t launch_kernel3( cudaStream_t, const TileItem *, int, const RunDev *, int, int, float, float, float, int );
-cudaError_t launch_shift_left( cudaStream_t, const TileItem *, int, const RunDev *, int, int );
+cudaError_t launch_shift_left( cudaStream_t, const TileItem *, int, const RunDev *, int );
 cudaError_t launch_field_energy( cudaStream_t, const RunDev *, int, int, double * );
 cudaError_t launch_grid_add( cudaStream_t, float *, const float *, size_t );
 cudaError_t launch_charge_finish( cudaStream_t, const float *, float *, int, int, int, int, int, int, int, int );
@@ -182,6 +182,7 @@ struct Plan {
     TileItem * tile_items_d = nullptr; int n_tiles = 0;
     int max_tile_vol = 0;
     int max_cells = 0, max_guard = 0;   // cells and guard cells of the largest tile
+    int max_nxy = 0;                // tile rows (cells in y) of the tallest tile
     int jacc = 0;                   // tile current accumulation (option "jacc")
     int tile_n = 0;                 // n when every run has n x n tiles with a specialised kernel
     int max_tile_cells = 0;         // cells of the largest tile (without guard cells)
@@ -364,7 +365,7 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
     P.sps_h.clear(); P.sp_sim.clear(); P.sp_local.clear();
     P.sp_k1_off.clear(); P.sp_k1_n.clear(); P.sp_sort_off.clear(); P.sp_sort_n.clear();
     P.max_tile_vol = 0;
-    P.max_cells = 0; P.max_guard = 0; P.max_tile_cells = 0;
+    P.max_cells = 0; P.max_guard = 0; P.max_tile_cells = 0; P.max_nxy = 0;
     P.reorder_every = 0; P.reorder_count = 0;
     P.jacc = -1;
     P.tile_n = -1;
@@ -382,6 +383,7 @@ static int plan_build( Plan & P, const std::vector<zpic_sim *> & sims, int chunk
         P.max_cells = std::max( P.max_cells, s->run.extx * s->run.exty );
         P.max_guard = std::max( P.max_guard, s->run.extx * s->run.exty - s->run.nxx * s->run.nxy );
         P.max_tile_cells = std::max( P.max_tile_cells, s->run.nxx * s->run.nxy );
+        P.max_nxy = std::max( P.max_nxy, s->run.nxy );
         // a batch reorders as often as its most frequent run asks
         const int every = s->reorder_every >= 0 ? s->reorder_every : ( s->emf_mw.active ? 0 : REORDER_AUTO_STEPS );
         if ( every > 0 )
@@ -572,19 +574,20 @@ static int run_current( Plan & P, cudaStream_t st ) {
 }
 
 // EMF::advance device part (emf.cpp:513-580 and 135-194): Yee, guard cells, bc.
-// before_shift: a window shift of a run without physical boundaries follows
-// at once; the Yee kernel saves the first interior column of B for it and
-// the guard refresh is left to the shift (run_shift's from_yee).
-static int run_fields( Plan & P, cudaStream_t st, int with_j, int j_raw, int clear_jdep, bool before_shift = false ) {
-    if ( before_shift ) {
-        PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 1 );
+// with_shift: EMF::move_window (emf.cpp:120-129) follows at once in a run
+// without physical boundaries; the Yee kernel writes its tiles shifted and
+// the guard refresh completes the shift (two kernels instead of four).
+static int run_fields( Plan & P, cudaStream_t st, int with_j, int j_raw, int clear_jdep, bool with_shift = false ) {
+    if ( with_shift ) {
+        PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 2 );
         DEV( launch_yee( st, P.tile_items_d, P.n_tiles, P.runs_d, with_j, j_raw, clear_jdep, P.max_tile_vol, 1 ) );
+        DEV( launch_emf_gc( st, P.tile_items_d, P.n_tiles, P.runs_d, 3, P.max_guard, P.max_nxy ) );
         return ZPIC_OK;
     }
     {
         PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 2 );
         DEV( launch_yee( st, P.tile_items_d, P.n_tiles, P.runs_d, with_j, j_raw, clear_jdep, P.max_tile_vol, 0 ) );
-        DEV( launch_emf_gc( st, P.tile_items_d, P.n_tiles, P.runs_d, 3, P.max_guard ) );
+        DEV( launch_emf_gc( st, P.tile_items_d, P.n_tiles, P.runs_d, 3, P.max_guard, 0 ) );
     }
     if ( !P.needs_bc_or_filter ) return ZPIC_OK;
     for ( size_t r = 0; r < P.sims.size(); r++ ) {
@@ -601,16 +604,14 @@ static int run_fields( Plan & P, cudaStream_t st, int with_j, int j_raw, int cle
     return ZPIC_OK;
 }
 
-// EMF::move_window (emf.cpp:120-129) for one run of the plan.  from_yee:
-// straight after run_fields( ..., before_shift ), whose guard refresh the
-// shift's (both axes instead of x) replaces.
-static int run_shift( Plan & P, cudaStream_t st, int r, bool from_yee = false ) {
+// EMF::move_window (emf.cpp:120-129) for one run of the plan
+static int run_shift( Plan & P, cudaStream_t st, int r ) {
     int first = 0;
     for ( int q = 0; q < r; q++ ) first += P.sims[q]->ntx * P.sims[q]->nty;
     const int nt = P.sims[r]->ntx * P.sims[r]->nty;
     PhaseScope ps( prof_sim( P ), st, PH_FIELDS, 2 );
-    DEV( launch_shift_left( st, P.tile_items_d + first, nt, P.runs_d, P.max_tile_vol, from_yee ? 1 : 0 ) );
-    DEV( launch_emf_gc( st, P.tile_items_d + first, nt, P.runs_d, from_yee ? 3 : 1, P.max_guard ) );
+    DEV( launch_shift_left( st, P.tile_items_d + first, nt, P.runs_d, P.max_tile_vol ) );
+    DEV( launch_emf_gc( st, P.tile_items_d + first, nt, P.runs_d, 1, P.max_guard, 0 ) );
     return ZPIC_OK;
 }
 
@@ -1488,10 +1489,12 @@ static int mw_step( zpic_sim * s ) {
     TRY( run_current( P, P.side ) );
     s->cur_iter++;
     if ( s->cur_mw.needs_move( s->cur_iter * s->dt ) ) s->cur_mw.advance();
-    // a window shift right after the field solve takes over its guard refresh
+    // a window shift right after the field solve is folded into it (the Yee
+    // kernel writes its tiles shifted, one guard refresh completes the shift)
     // when no physical boundary has to be applied in between and every y
-    // guard cell has a source (periodic y): then the guard cells come out
-    // the same as with the two refreshes
+    // guard cell has a source (periodic y): then every field value, guard
+    // cells included, comes out as with the solve and the shift one after
+    // the other
     const bool shift = s->emf_mw.active && s->emf_mw.needs_move( ( s->emf_iter + 1 ) * s->dt );
     bool fused = shift && P.sims.size() == 1 && s->run.emf_pery;
     for ( int k = 0; k < 4; k++ ) fused = fused && s->emf_bc[k] <= ZPIC_EMF_BC_PERIODIC;
@@ -1500,7 +1503,7 @@ static int mw_step( zpic_sim * s ) {
     s->j_final = true;
     s->emf_iter++;
     if ( shift ) {
-        TRY( run_shift( P, P.side, 0, fused ) );
+        if ( !fused ) TRY( run_shift( P, P.side, 0 ) );
         s->emf_mw.advance();
     }
     DEV( cudaEventRecord( P.join, P.side ) );

@@ -130,17 +130,40 @@ k_current_gc( const TileItem * __restrict__ items, const RunDev * __restrict__ r
     }
 }
 
-// grid::copy_to_gc on E and B in place (axes: 1 x, 2 y, 3 both)
+// the tile right of (tx, ty) for E and B, or -1
+__device__ __forceinline__ int right_tile( const RunDev & R, int tx, int ty ) {
+    const int n = nbr( tx + 1, R.ntx, R.emf_perx );
+    return n >= 0 ? ty * R.ntx + n : -1;
+}
+
+// grid::copy_to_gc on E and B in place (axes: 1 x, 2 y, 3 both).
+// bfix: after a Yee kernel that wrote its tile shifted one cell to the left
+// (shift_out), B of every tile's new last interior column is the right
+// neighbour's first interior column saved in bcol (where there is a right
+// neighbour): the threads after the guard cells of a tile write it, and guard
+// cells whose source is such a cell read it from bcol as well.
 __global__ void __launch_bounds__( GC_THREADS )
-k_emf_gc( const TileItem * __restrict__ items, int nitems, int per, const RunDev * __restrict__ runs, int axes )
+k_emf_gc( const TileItem * __restrict__ items, int nitems, int per, const RunDev * __restrict__ runs, int axes,
+          int bfix )
 {
     const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x;     // n * per < 2^31 (launcher)
     const int w = (int) ( gid / (unsigned) per ), g = (int) ( gid % (unsigned) per );
     if ( w >= nitems ) return;
     const TileItem it = items[w];
     const RunDev & R = runs[ it.run ];
-    if ( g >= guard_count( R ) ) return;
     const int tx = it.tile % R.ntx, ty = it.tile / R.ntx;
+    const int ng = guard_count( R );
+    if ( g >= ng ) {
+        const int row = g - ng;
+        if ( !bfix || row >= R.nxy ) return;
+        const int rn = right_tile( R, tx, ty );
+        if ( rn < 0 ) return;
+        const size_t dst = ( (size_t) it.tile * R.tile_vol + ( GL + row ) * R.extx + GL + R.nxx - 1 ) * 3;
+        const float * b = R.bcol + ( (size_t) rn * R.nxy + row ) * 3;
+        const float b0 = b[0], b1 = b[1], b2 = b[2];
+        R.B[dst] = b0; R.B[dst + 1] = b1; R.B[dst + 2] = b2;
+        return;
+    }
     int i, j;
     guard_cell( g, R, i, j );
     int stx, sty, si, sj;
@@ -149,6 +172,10 @@ k_emf_gc( const TileItem * __restrict__ items, int nitems, int per, const RunDev
     const size_t dst = ( (size_t) it.tile * R.tile_vol + j * R.extx + i ) * 3;
     const float * e = cellp( R.E, R, stx, sty, si, sj );
     const float * b = cellp( R.B, R, stx, sty, si, sj );
+    if ( bfix && si == GL + R.nxx - 1 && sj >= GL && sj < GL + R.nxy ) {
+        const int rn = right_tile( R, stx, sty );
+        if ( rn >= 0 ) b = R.bcol + ( (size_t) rn * R.nxy + sj - GL ) * 3;
+    }
     const float e0 = e[0], e1 = e[1], e2 = e[2], b0 = b[0], b1 = b[1], b2 = b[2];
     R.E[dst] = e0; R.E[dst + 1] = e1; R.E[dst + 2] = e2;
     R.B[dst] = b0; R.B[dst + 1] = b1; R.B[dst + 2] = b2;
@@ -217,7 +244,7 @@ __device__ __forceinline__ void yee_e_smem( float * E, const float * B, const fl
 
 __global__ void __launch_bounds__( YEE_THREADS )
 k_yee( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, int with_j, int j_raw, int clear_jdep,
-       int save_bcol )
+       int shift_out )
 {
     extern __shared__ __align__( 16 ) unsigned char smem_raw[];
     const TileItem it = items[ blockIdx.x ];
@@ -252,24 +279,37 @@ k_yee( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, in
     yee_b_smem( E0, B0, R, R.dtx2, R.dty2 );
     __syncthreads();
 
-    if ( threadIdx.x == 0 ) {
-        fence_proxy_async_smem();
-        bulk_s2g( R.E + toff, sE, bytes );
-        bulk_s2g( R.B + toff, sB, bytes );
-        bulk_commit();
+    if ( !shift_out ) {
+        if ( threadIdx.x == 0 ) {
+            fence_proxy_async_smem();
+            bulk_s2g( R.E + toff, sE, bytes );
+            bulk_s2g( R.B + toff, sB, bytes );
+            bulk_commit();
+        }
+    } else {
+        // a window shift (grid::x_shift_left(1)) follows at once: the tile is
+        // written one cell to the left, the last cell of every row cleared.
+        // The new last interior column is the first upper guard column: E
+        // there is this kernel's own update of it, bit for bit the right
+        // neighbour's (same inputs, same arithmetic); B there would need E one
+        // column further out, so the right neighbour's first interior column
+        // of B is saved (bcol) and put in place by the guard refresh that
+        // follows (k_emf_gc, bfix), which also refreshes every guard cell.
+        const int ys = R.extx, nc = 3 * R.extx * R.exty;
+        for ( int f = threadIdx.x; f < 2 * nc; f += blockDim.x ) {
+            const int fld = f >= nc, e = f - fld * nc;
+            const int ix = ( e / 3 ) % ys;
+            ( fld ? R.B : R.E )[ toff + e ] = ( ix < ys - 1 ) ? ( fld ? sB : sE )[ e + 3 ] : 0.0f;
+        }
+        float * dst = R.bcol + (size_t) it.tile * R.nxy * 3;
+        for ( int q = threadIdx.x; q < 3 * R.nxy; q += blockDim.x ) dst[q] = B0[ 3 * ( ( q / 3 ) * R.extx ) + q % 3 ];
     }
     if ( clear_jdep ) {
         float4 * z = reinterpret_cast<float4 *>( R.Jdep + toff );
         for ( int i = threadIdx.x; i < 3 * tv / 4; i += blockDim.x ) z[i] = make_float4( 0.f, 0.f, 0.f, 0.f );
     }
-    if ( save_bcol ) {
-        // B of the first interior column, for the window shift that follows
-        // (the left neighbour's new last interior column)
-        float * dst = R.bcol + (size_t) it.tile * R.nxy * 3;
-        for ( int q = threadIdx.x; q < 3 * R.nxy; q += blockDim.x ) dst[q] = B0[ 3 * ( ( q / 3 ) * R.extx ) + q % 3 ];
-    }
     // the shared-memory sources read; the stores complete before the kernel does
-    if ( threadIdx.x == 0 ) bulk_wait_read_all();
+    if ( threadIdx.x == 0 && !shift_out ) bulk_wait_read_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -485,7 +525,7 @@ k_kernel3( const TileItem * __restrict__ items, const RunDev * __restrict__ runs
 constexpr int SHIFT_THREADS = 256;
 
 __global__ void __launch_bounds__( SHIFT_THREADS )
-k_shift_left( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, int from_yee )
+k_shift_left( const TileItem * __restrict__ items, const RunDev * __restrict__ runs )
 {
     extern __shared__ __align__( 16 ) float sA[];   // [E block][B block]
     const TileItem it = items[ blockIdx.x ];
@@ -500,24 +540,6 @@ k_shift_left( const TileItem * __restrict__ items, const RunDev * __restrict__ r
     }
     __syncthreads();
     const int ys = R.extx, nc = 3 * R.extx * R.exty;
-    if ( from_yee ) {
-        // Straight after the Yee kernel, before any guard refresh.  The new
-        // last interior column takes the first upper guard column: E there is
-        // the Yee kernel's own update of that column, bit for bit the right
-        // neighbour's (same inputs, same arithmetic), but B there needs E one
-        // column further out, so B's guard column is replaced by the right
-        // neighbour's saved first interior column (bcol); without a right
-        // neighbour the guard is kept, as a guard refresh would.  Every guard
-        // cell is refreshed afterwards (axes 3).
-        const int tx = it.tile % R.ntx, ty = it.tile / R.ntx;
-        const int rn = tx + 1 < R.ntx ? tx + 1 : ( R.emf_perx ? 0 : -1 );
-        if ( rn >= 0 ) {
-            const float * src = R.bcol + (size_t) ( ty * R.ntx + rn ) * R.nxy * 3;
-            for ( int q = threadIdx.x; q < 3 * R.nxy; q += SHIFT_THREADS )
-                sA[ n + 3 * ( ( q / 3 + 1 ) * ys + R.nxx + 1 ) + q % 3 ] = src[q];
-            __syncthreads();
-        }
-    }
 #pragma unroll 4
     for ( int f = threadIdx.x; f < 2 * nc; f += SHIFT_THREADS ) {
         const int fld = f >= nc, e = f - fld * nc;    // float e of cell e / 3 in the field's block
@@ -620,9 +642,11 @@ cudaError_t launch_current_gc( cudaStream_t st, const TileItem * items, int n, c
     if ( n > 0 ) k_current_gc<<< n, 128, 0, st >>>( items, runs );
     return cudaGetLastError();
 }
-cudaError_t launch_emf_gc( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int axes, int per ) {
+cudaError_t launch_emf_gc( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int axes, int per,
+                           int bfix_rows ) {
+    per += bfix_rows;
     if ( !gc_fits( n, per ) ) return cudaErrorInvalidConfiguration;
-    if ( n > 0 ) k_emf_gc<<< gc_blocks( n, per ), GC_THREADS, 0, st >>>( items, n, per, runs, axes );
+    if ( n > 0 ) k_emf_gc<<< gc_blocks( n, per ), GC_THREADS, 0, st >>>( items, n, per, runs, axes, bfix_rows > 0 );
     return cudaGetLastError();
 }
 cudaError_t launch_cur_gc( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int axes, int per ) {
@@ -631,10 +655,10 @@ cudaError_t launch_cur_gc( cudaStream_t st, const TileItem * items, int n, const
     return cudaGetLastError();
 }
 cudaError_t launch_yee( cudaStream_t st, const TileItem * items, int n, const RunDev * runs,
-                        int with_j, int j_raw, int clear_jdep, int max_tile_vol, int save_bcol ) {
+                        int with_j, int j_raw, int clear_jdep, int max_tile_vol, int shift_out ) {
     const size_t smem = yee_smem_bytes( max_tile_vol );
     if ( smem > 48 * 1024 ) cudaFuncSetAttribute( (const void *) k_yee, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
-    if ( n > 0 ) k_yee<<< n, YEE_THREADS, smem, st >>>( items, runs, with_j, j_raw, clear_jdep, save_bcol );
+    if ( n > 0 ) k_yee<<< n, YEE_THREADS, smem, st >>>( items, runs, with_j, j_raw, clear_jdep, shift_out );
     return cudaGetLastError();
 }
 cudaError_t launch_emf_bc( cudaStream_t st, const RunDev * runs, int run, int axis, int nthreads ) {
@@ -652,11 +676,10 @@ cudaError_t launch_kernel3( cudaStream_t st, const TileItem * items, int n, cons
     if ( n > 0 ) k_kernel3<<< n, 128, smem, st >>>( items, runs, which, diry, a, b, c );
     return cudaGetLastError();
 }
-cudaError_t launch_shift_left( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int max_tile_vol,
-                               int from_yee ) {
+cudaError_t launch_shift_left( cudaStream_t st, const TileItem * items, int n, const RunDev * runs, int max_tile_vol ) {
     const size_t smem = (size_t) 6 * max_tile_vol * sizeof( float );
     if ( smem > 48 * 1024 ) cudaFuncSetAttribute( (const void *) k_shift_left, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
-    if ( n > 0 ) k_shift_left<<< n, SHIFT_THREADS, smem, st >>>( items, runs, from_yee );
+    if ( n > 0 ) k_shift_left<<< n, SHIFT_THREADS, smem, st >>>( items, runs );
     return cudaGetLastError();
 }
 cudaError_t launch_field_energy( cudaStream_t st, const RunDev * runs, int run, int ntiles, double * out ) {
