@@ -279,37 +279,41 @@ k_yee( const TileItem * __restrict__ items, const RunDev * __restrict__ runs, in
     yee_b_smem( E0, B0, R, R.dtx2, R.dty2 );
     __syncthreads();
 
-    if ( !shift_out ) {
-        if ( threadIdx.x == 0 ) {
-            fence_proxy_async_smem();
-            bulk_s2g( R.E + toff, sE, bytes );
-            bulk_s2g( R.B + toff, sB, bytes );
-            bulk_commit();
-        }
-    } else {
+    const float * outE = sE, * outB = sB;
+    if ( shift_out ) {
         // a window shift (grid::x_shift_left(1)) follows at once: the tile is
-        // written one cell to the left, the last cell of every row cleared.
-        // The new last interior column is the first upper guard column: E
-        // there is this kernel's own update of it, bit for bit the right
-        // neighbour's (same inputs, same arithmetic); B there would need E one
-        // column further out, so the right neighbour's first interior column
-        // of B is saved (bcol) and put in place by the guard refresh that
-        // follows (k_emf_gc, bfix), which also refreshes every guard cell.
-        const int ys = R.extx, nc = 3 * R.extx * R.exty;
-        for ( int f = threadIdx.x; f < 2 * nc; f += blockDim.x ) {
-            const int fld = f >= nc, e = f - fld * nc;
-            const int ix = ( e / 3 ) % ys;
-            ( fld ? R.B : R.E )[ toff + e ] = ( ix < ys - 1 ) ? ( fld ? sB : sE )[ e + 3 ] : 0.0f;
-        }
+        // stored one cell to the left, the last cell of every row cleared --
+        // E shifted into the current tile's place (free after the E step),
+        // then B into E's.  The new last interior column is the first upper
+        // guard column: E there is this kernel's own update of it, bit for bit
+        // the right neighbour's (same inputs, same arithmetic); B there would
+        // need E one column further out, so the first interior column of B is
+        // saved (bcol) and the guard refresh that follows (k_emf_gc, bfix)
+        // puts the right neighbour's in place, refreshing every guard cell.
         float * dst = R.bcol + (size_t) it.tile * R.nxy * 3;
         for ( int q = threadIdx.x; q < 3 * R.nxy; q += blockDim.x ) dst[q] = B0[ 3 * ( ( q / 3 ) * R.extx ) + q % 3 ];
+        const int ys = R.extx, nc = 3 * R.extx * R.exty;
+        float * sT = sJ;
+        for ( int e = threadIdx.x; e < 3 * tv; e += blockDim.x )
+            sT[e] = e < nc ? ( ( ( e / 3 ) % ys < ys - 1 ) ? sE[ e + 3 ] : 0.0f ) : sE[e];
+        __syncthreads();
+        for ( int e = threadIdx.x; e < 3 * tv; e += blockDim.x )
+            sE[e] = e < nc ? ( ( ( e / 3 ) % ys < ys - 1 ) ? sB[ e + 3 ] : 0.0f ) : sB[e];
+        __syncthreads();
+        outE = sT; outB = sE;
+    }
+    if ( threadIdx.x == 0 ) {
+        fence_proxy_async_smem();
+        bulk_s2g( R.E + toff, outE, bytes );
+        bulk_s2g( R.B + toff, outB, bytes );
+        bulk_commit();
     }
     if ( clear_jdep ) {
         float4 * z = reinterpret_cast<float4 *>( R.Jdep + toff );
         for ( int i = threadIdx.x; i < 3 * tv / 4; i += blockDim.x ) z[i] = make_float4( 0.f, 0.f, 0.f, 0.f );
     }
     // the shared-memory sources read; the stores complete before the kernel does
-    if ( threadIdx.x == 0 && !shift_out ) bulk_wait_read_all();
+    if ( threadIdx.x == 0 ) bulk_wait_read_all();
 }
 
 // ---------------------------------------------------------------------------
